@@ -1,0 +1,126 @@
+/*
+ * xfmm.h -- C ABI of libexafmm_b200.so, the B200 (sm_100a) implementation of
+ * exafmm-t's kernel-independent FMM evaluate path.
+ *
+ * The entry points replace, one for one, the reference's C++ API for this path
+ * (namespace exafmm_t; file:line citations are relative to the exafmm-t tree):
+ *
+ *   xfmm_fmm_create      LaplaceFmm(p, ncrit, filename)                 include/laplace.h:15-22
+ *                        ModifiedHelmholtzFmm(p, ncrit, wavek, filename)include/modified_helmholtz.h:17-25
+ *                        HelmholtzFmm(p, ncrit, wavek, filename)        include/helmholtz.h:16-24
+ *   xfmm_build_tree      get_bounds + build_tree + balance_tree         include/build_tree.h:20-35, 181-199, 336-359
+ *                        (uniform variant)                              include/build_non_adaptive_tree.h:17-194
+ *   xfmm_build_list      init_rel_coord + set_colleagues + build_list   include/geometry.h:198-215,
+ *                                                                       include/build_list.h:123-197
+ *   xfmm_m2l_setup       Fmm::M2L_setup                                 include/fmm_scale_invariant.h:277-341, fmm.h:265-333
+ *   xfmm_precompute      Fmm::precompute                                include/fmm_scale_invariant.h:151-160, fmm.h:141-153
+ *   xfmm_set_charges     update_charges                                 python/exafmm.cpp:275-305
+ *   xfmm_upward_pass     FmmBase::upward_pass                           include/fmm_base.h:162-171
+ *   xfmm_downward_pass   FmmBase::downward_pass                         include/fmm_base.h:179-200
+ *   xfmm_get_values      result scatter of evaluate                     python/exafmm.cpp:190-267
+ *   xfmm_evaluate        clear_values + upward + downward + scatter     python/exafmm.cpp:190-267, 313-323
+ *   xfmm_gradient_p2p    <Kernel>Fmm::gradient_P2P                      include/laplace.h:91-164 (and twins)
+ *   xfmm_verify          FmmBase::verify                                include/fmm_base.h:208-267
+ *
+ * Conventions
+ *   - Every function returns an xfmm_status; xfmm_last_error() gives the message
+ *     of the last failure on the calling thread.  No C++ exception crosses the ABI.
+ *   - Coordinates are FP64, interleaved (x0,y0,z0,x1,...).  Charges and results are
+ *     FP64 reals (Laplace, modified Helmholtz) or interleaved FP64 complex pairs
+ *     (Helmholtz).  Results are (ntrg, 4): potential, d/dx, d/dy, d/dz, in the
+ *     caller's original target order.
+ *   - `on_device` != 0 means the pointer is device memory on the current device;
+ *     otherwise it is host memory and the call copies it (stream-ordered, then
+ *     synchronises for host outputs).
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  All device work
+ *     of a call is ordered on that stream.
+ *   - The library holds no global mutable state: different handles may be used
+ *     from different host threads concurrently; one handle must not be.
+ */
+#ifndef XFMM_H
+#define XFMM_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  XFMM_OK = 0,
+  XFMM_ERR_ARG = 1,         /* invalid argument / shape (python/exafmm.cpp:37-40 analogue) */
+  XFMM_ERR_OOM = 2,         /* device or host allocation failed */
+  XFMM_ERR_CUDA = 3,        /* a CUDA runtime or library call failed */
+  XFMM_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
+  XFMM_ERR_STATE = 5,       /* call order violated (e.g. evaluate before precompute) */
+  XFMM_ERR_UNSUPPORTED = 6, /* configuration outside the implemented range */
+  XFMM_ERR_NUMERIC = 7      /* non-finite input or a failed factorisation */
+} xfmm_status;
+
+typedef enum { XFMM_LAPLACE = 0, XFMM_MODIFIED_HELMHOLTZ = 1, XFMM_HELMHOLTZ = 2 } xfmm_kernel;
+
+/* Arithmetic of the evaluate path.
+ *   XFMM_FP64  : every stage in FP64, operators as the reference (pinv threshold 4e-16*smax).
+ *   XFMM_MIXED : FP32 near field (FP64-accumulated per source tile), FP32 FFT/Hadamard M2L,
+ *                FP32 translations; operators precomputed in FP64 with the check-to-equivalent
+ *                pinv regularised at 4e-10*smax so FP32 equivalent densities lose nothing. */
+typedef enum { XFMM_FP64 = 0, XFMM_MIXED = 1 } xfmm_precision;
+
+typedef struct xfmm_fmm xfmm_fmm;
+typedef struct xfmm_tree xfmm_tree;
+
+const char* xfmm_last_error(void);
+const char* xfmm_version(void);
+
+/* Fmm object: kernel, expansion order p (2..16), ncrit, wavenumber, precision. */
+xfmm_status xfmm_fmm_create(int kernel, int p, int ncrit, double k_re, double k_im, int precision, xfmm_fmm** out);
+xfmm_status xfmm_fmm_free(xfmm_fmm* fmm);
+/* Public fields of FmmBase (fmm_base.h:13-23): p, nsurf, nconv, nfreq, ncrit, depth, and x0[3], r0. */
+xfmm_status xfmm_fmm_info(const xfmm_fmm* fmm, int64_t* ints6, double* x0r0_4);
+
+/* Tree over device-resident bodies.  nonadaptive_depth < 0: adaptive tree + 2:1 balance
+ * (python/exafmm.cpp:129-140); >= 0: uniform tree to that depth (NON_ADAPTIVE build).
+ * Sets fmm->x0, r0 and depth exactly as get_bounds/balance_tree do. */
+xfmm_status xfmm_build_tree(xfmm_fmm* fmm, const double* src_xyz, int64_t nsrc, const double* trg_xyz, int64_t ntrg,
+                            int nonadaptive_depth, int on_device, void* stream, xfmm_tree** out);
+xfmm_status xfmm_tree_free(xfmm_tree* tree);
+xfmm_status xfmm_build_list(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
+xfmm_status xfmm_m2l_setup(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
+xfmm_status xfmm_precompute(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
+
+/* Charges in the caller's original source order (nsrc reals, or nsrc complex pairs). */
+xfmm_status xfmm_set_charges(xfmm_fmm* fmm, xfmm_tree* tree, const double* q, int on_device, void* stream);
+xfmm_status xfmm_clear_values(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
+xfmm_status xfmm_upward_pass(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
+xfmm_status xfmm_downward_pass(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
+xfmm_status xfmm_get_values(xfmm_fmm* fmm, xfmm_tree* tree, double* out, int on_device, void* stream);
+/* clear_values + upward_pass + downward_pass + get_values. */
+xfmm_status xfmm_evaluate(xfmm_fmm* fmm, xfmm_tree* tree, double* out, int on_device, void* stream);
+
+/* Tree statistics: nnodes, nleafs, nnonleafs, depth, np2p, nm2p, np2l, n_m2l_src,
+ * p2p_pairs, m2p_pairs, l2p_pairs, m2l_pairs (12 int64). */
+xfmm_status xfmm_tree_info(const xfmm_tree* tree, int64_t* info12);
+/* Flat dump of the tree and lists in the reference's node order; array shapes as
+ * oracle/ref_capi.cpp's ref_dump (nnodes from xfmm_tree_info).  Host pointers. */
+xfmm_status xfmm_tree_dump(const xfmm_tree* tree, double* geo, uint64_t* key, int32_t* ni, double* nx, int32_t* leafs,
+                           int32_t* nonleafs, int32_t* src_perm, int32_t* trg_perm, int32_t* colleagues,
+                           int32_t* m2l, int64_t* p2p_off, int32_t* p2p, int64_t* m2p_off, int32_t* m2p,
+                           int64_t* p2l_off, int32_t* p2l);
+/* Per-stage device times (ms) of the last evaluate: P2M, M2M, P2L, M2P+L2P, P2P, M2L, L2L, total;
+ * and the M2L sub-stages FFT, Hadamard, iFFT (11 doubles). */
+xfmm_status xfmm_stage_times(const xfmm_fmm* fmm, double* ms11);
+
+/* Direct near-field kernel over raw arrays: out (ntrg x 4) += potential and gradient
+ * at trg from (src, q).  precision selects the FP64 or FP32 device kernel. */
+xfmm_status xfmm_gradient_p2p(int kernel, double k_re, double k_im, int precision, const double* src_xyz,
+                              int64_t nsrc, const double* q, const double* trg_xyz, int64_t ntrg, double* out,
+                              int on_device, void* stream);
+
+/* FmmBase::verify on the device: relative L2 error of potential and gradient of the last
+ * evaluate against FP64 direct summation over all sources, on every target (sample == 0)
+ * or the targets of 10 leaves at stride nleafs/10 (sample != 0). */
+xfmm_status xfmm_verify(xfmm_fmm* fmm, xfmm_tree* tree, int sample, double* err2, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -181,11 +181,10 @@ def potential_matrix(kernel, wavek, src, trg):
 class Operators:
     """Check-to-equivalent pinv factors, M2M/L2L and M2L tables for one level (FP64)."""
 
-    def __init__(self, kernel, wavek, p, r0, level, m2l_level=None):
+    def __init__(self, kernel, wavek, p, r0, level, m2l_level=None, eps=1e-16):
         self.kernel, self.wavek, self.p = kernel, wavek, p
         n = nsurf_of(p)
         cplx = kernel == "helmholtz"
-        eps = 1e-16
         c = np.zeros(3)
         up_check = surface(p, r0, level, c, 2.95)
         up_equiv = surface(p, r0, level, c, 1.05)
@@ -251,7 +250,8 @@ def m2l_tables(kernel, wavek, p, r0, l):
 class NpFmm:
     """Reference-semantics FMM on the oracle tree.  ``evaluate`` returns (ntrg, 4) in input order."""
 
-    def __init__(self, kernel, p, ncrit, wavek=0.0, nonadaptive_depth=None, emulate=None):
+    def __init__(self, kernel, p, ncrit, wavek=0.0, nonadaptive_depth=None, emulate=None, pinv_eps=1e-16):
+        self.pinv_eps = pinv_eps
         assert kernel in KERNELS
         self.kernel, self.p, self.ncrit = kernel, p, ncrit
         self.wavek = complex(wavek)
@@ -288,10 +288,11 @@ class NpFmm:
         self.sq = self.q[t["src_perm"]]
         wk = self.wavek
         if self.kernel == "laplace":
-            self.ops = {0: Operators(self.kernel, wk, self.p, self.r0, 0, m2l_level=0)}
+            self.ops = {0: Operators(self.kernel, wk, self.p, self.r0, 0, m2l_level=0, eps=self.pinv_eps)}
         else:
             self.ops = {l: Operators(self.kernel, wk, self.p, self.r0, l,
-                                     m2l_level=l if l >= 1 else None) for l in range(self.depth + 1)}
+                                     m2l_level=l if l >= 1 else None, eps=self.pinv_eps)
+                        for l in range(self.depth + 1)}
         return self
 
     def _op(self, level):

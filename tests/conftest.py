@@ -18,3 +18,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 @pytest.fixture(scope="session")
 def golden_dir():
     return GOLDEN
+
+PKG = os.path.join(ROOT, "exafmm-t_b200")
+if PKG not in sys.path:
+    sys.path.insert(0, PKG)

@@ -1,0 +1,120 @@
+"""Parity of the CUDA path (through the C ABI) with the reference, on a B200.
+
+Integer/tree work is compared bit for bit with fixtures produced by the reference
+itself (tests/golden); FP64 potentials and gradients within 1e-9 relative L2 of the
+reference's own FMM; the mixed path within 5e-6 of the reference at p=4..6 (its own
+FMM truncation error dominates there) and against the FP64 direct-sum oracle."""
+import numpy as np
+import pytest
+
+from oracle import fmm_np, orc
+from tests.golden_cases import TREE_KEYS, case_names, load, load_p2p
+
+pytestmark = pytest.mark.gpu
+
+CASES = case_names()
+FP64_TOL = 1e-9     # FP64 GPU vs reference FMM (same algorithm, different SVD/FFT libraries and sum order)
+MIXED_TOL = 5e-6    # mixed GPU vs reference FMM at these small p
+
+
+def _mod(kernel):
+    import exafmm.helmholtz
+    import exafmm.laplace
+    import exafmm.modified_helmholtz
+    return {"laplace": exafmm.laplace, "helmholtz": exafmm.helmholtz,
+            "modified_helmholtz": exafmm.modified_helmholtz}[kernel]
+
+
+def _fmm(g, precision):
+    m = _mod(g["kernel"])
+    if g["kernel"] == "laplace":
+        return m.LaplaceFmm(g["p"], g["ncrit"], precision=precision)
+    if g["kernel"] == "helmholtz":
+        return m.HelmholtzFmm(g["p"], g["ncrit"], g["wavek"], precision=precision)
+    return m.ModifiedHelmholtzFmm(g["p"], g["ncrit"], g["wavek"].real, precision=precision)
+
+
+def _setup(g, precision):
+    m = _mod(g["kernel"])
+    fmm = _fmm(g, precision)
+    tree = m.setup(m.init_sources(g["src"], g["q"]), m.init_targets(g["trg"]), fmm,
+                   nonadaptive_depth=g["nonadaptive_depth"])
+    return m, fmm, tree
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_tree_and_lists_bit_exact(name):
+    g = load(name)
+    _, fmm, tree = _setup(g, "fp64")
+    d = tree.dump()
+    for k in TREE_KEYS:
+        assert np.array_equal(d[k], g["tree"][k]), k
+    assert d["depth"] == g["tree"]["depth"]
+    assert d["r0"] == g["tree"]["r0"]
+    assert fmm.depth == g["tree"]["depth"] and fmm.r0 == g["tree"]["r0"]
+
+
+@pytest.mark.parametrize("kernel,wk,qkey", [("laplace", 0.0, "q"), ("modified_helmholtz", 10.0, "q"),
+                                            ("helmholtz", 5.0 + 10.0j, "qc")])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("mixed", 2e-6)])
+def test_p2p_kernels_match_reference(kernel, wk, qkey, precision, tol):
+    g = load_p2p()
+    from exafmm import _core
+    out = _core.gradient_p2p(kernel, g["src"], g[qkey], g["trg"], wk, precision)
+    pe, ge = orc.rel_l2(out, g[kernel])
+    assert pe < tol and ge < tol, (pe, ge)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fmm_fp64_matches_reference(name):
+    g = load(name)
+    m, fmm, tree = _setup(g, "fp64")
+    out = m.evaluate(tree, fmm)
+    pe, ge = orc.rel_l2(out, g["out"])
+    assert pe < FP64_TOL and ge < FP64_TOL, (pe, ge)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fmm_mixed_matches_reference(name):
+    g = load(name)
+    m, fmm, tree = _setup(g, "mixed")
+    out = m.evaluate(tree, fmm)
+    pe, ge = orc.rel_l2(out, g["out"])
+    assert pe < MIXED_TOL and ge < MIXED_TOL, (pe, ge)
+
+
+def test_fmm_p8_against_oracle_and_direct():
+    rng = np.random.default_rng(11)
+    x = rng.random((20000, 3))
+    q = rng.uniform(-1, 1, 20000)
+    import exafmm.laplace as L
+    ref = fmm_np.NpFmm("laplace", 8, 128).setup(x, q, x).evaluate()
+    ex = orc.direct("laplace", x, q, x[:500])
+    for prec, tol in (("fp64", 1e-10), ("mixed", 1e-6)):
+        fmm = L.LaplaceFmm(8, 128, precision=prec)
+        tree = L.setup(L.init_sources(x, q), L.init_targets(x), fmm)
+        out = L.evaluate(tree, fmm)
+        if prec == "fp64":
+            pe, ge = orc.rel_l2(out, ref)
+            assert pe < tol and ge < tol, (prec, pe, ge)
+        pe, ge = orc.rel_l2(out[:500], ex)
+        assert pe < 1e-6 and ge < 3e-6, (prec, pe, ge)
+
+
+def test_update_charges_and_reevaluate():
+    g = load("laplace_cube_p4")
+    m, fmm, tree = _setup(g, "fp64")
+    out1 = m.evaluate(tree, fmm)
+    m.update_charges(tree, 2.0 * g["q"])
+    m.clear_values(tree)
+    out2 = m.evaluate(tree, fmm)
+    assert np.allclose(out2, 2.0 * out1, rtol=1e-12, atol=1e-12 * np.abs(out1).max())
+
+
+def test_verify_matches_oracle():
+    g = load("laplace_cube_p4")
+    m, fmm, tree = _setup(g, "fp64")
+    out = m.evaluate(tree, fmm)
+    e = fmm.verify(tree.leafs, sample=False)
+    pe, ge = orc.rel_l2(out, orc.direct("laplace", g["src"], g["q"], g["trg"]))
+    assert abs(e[0] - pe) < 1e-3 * pe and abs(e[1] - ge) < 1e-3 * ge
