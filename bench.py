@@ -1,0 +1,312 @@
+"""Benchmark: Laplace FMM evaluate, N=4,000,000 uniform in [0,1)^3, p=8, ncrit=128 (adaptive + 2:1
+balance), charges U[-1,1), seeds 0 (positions) / 1 (charges).
+
+One step = one evaluate (upward + downward pass) on the device-resident tree, i.e. the reference's
+upward_pass + downward_pass (include/fmm_base.h:162-200) on its own tree; setup (tree, lists,
+precompute) is timed separately.  The headline value is the mixed-precision path; the plain FP64
+GPU path is measured in the same run for the mixed/FP64 ratio, and both are checked against the
+FP64 direct-sum oracle on 1000 sampled targets (relative L2 of potential and gradient).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n N]
+
+--impl reference times the reference's own CPU implementation (the unmodified exafmm-t headers,
+built into oracle/_ref) on the host cores, on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "exafmm-t_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "Laplace N=4M p=8 Mparticles/s: mixed vs FP64 GPU at L2 err ≤1e-6; fwd+bwd time"
+P, NCRIT = 8, 128
+FLOPS_PER_P2P_PAIR = 28  # the reference's count for gradient P2P (laplace.h:163)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n):
+    x = np.random.default_rng(0).random((n, 3))
+    q = np.random.default_rng(1).uniform(-1.0, 1.0, n)
+    return x, q
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu=0):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d, "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def run_ours(args, rank, world):
+    import torch
+    import exafmm.laplace as L
+    from exafmm import _lib
+
+    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
+    n = args.n
+    x, q = workload(n)  # every rank evaluates its own replica of the workload (weak scaling)
+    res = {}
+    paths = ["mixed"] + ([] if args.no_fp64 else ["fp64"])
+    outs = {}
+    for prec in paths:
+        fmm = L.LaplaceFmm(P, NCRIT, precision=prec)
+        t0 = time.perf_counter()
+        tree = L.setup(L.init_sources(x, q), L.init_targets(x), fmm)
+        torch.cuda.synchronize()
+        setup_s = time.perf_counter() - t0
+        info = tree.info()
+        lib = _lib.lib()
+        dev_out = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+        op, _ = _lib.ptr(dev_out)
+        st = _lib.ctypes.c_void_p(0)
+
+        def step():
+            _lib.check(lib.xfmm_evaluate(fmm._h, tree._h, op, 1, st))
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stage_acc = None
+        with ClockSampler(rank) as clk:
+            e0.record()
+            for _ in range(args.steps):
+                step()
+            e1.record()
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        # per-stage device times of one more step (CUDA events inside the library)
+        step()
+        stage_acc = fmm.stage_times(tree)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        outs[prec] = dev_out.cpu().numpy()
+        # end to end through the public API with HOST buffers (pinned): update_charges copies the
+        # charges host->device, evaluate runs both passes and copies the (N, 4) result device->host
+        q_host = torch.from_numpy(q.copy()).pin_memory().numpy()
+        out_host = torch.empty((n, 4), dtype=torch.float64).pin_memory().numpy()
+
+        def e2e_step():
+            L.update_charges(tree, q_host)
+            L.evaluate(tree, fmm, out=out_host)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        k2 = max(3, args.steps // 2)
+        t0 = time.perf_counter()
+        for _ in range(k2):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / k2
+        res[prec] = dict(ms=ms, setup_s=setup_s, info=info, stages=stage_acc, clocks=clk.summary(), e2e_ms=e2e_ms)
+        del tree, fmm, dev_out
+        torch.cuda.empty_cache()
+    return res, outs, x, q
+
+
+def accuracy(outs, x, q):
+    from oracle import orc
+    samp = np.random.default_rng(2).choice(len(x), 1000, replace=False)
+    ex = orc.direct("laplace", x, q, x[samp])
+    return {k: dict(zip(("potential", "gradient"), orc.rel_l2(v[samp], ex))) for k, v in outs.items()}
+
+
+def roofline(r, peaks, src):
+    """Dominant kernels: target evaluation (FP32 SIMT FLOP/s) and the M2L Hadamard (HBM bytes)."""
+    info, st = r["info"], r["stages"]
+    n = 8  # children per node
+    nfreq = (2 * P) ** 2 * (P + 1)
+    # M2L Hadamard algorithmic bytes: spectra in (sources) + out (targets) + 26 tables, complex64
+    had_bytes = (info["n_m2l_src"] + info["nnonleafs"]) * n * nfreq * 8 + 26 * nfreq * 64 * 8
+    had_ms = st["M2L_hadamard"]
+    sm_mhz = r["clocks"].get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s, FMA = 2 flops
+    pairs = info["p2p_pairs"] + info["m2p_pairs"] + info["l2p_pairs"]
+    eval_tflops = pairs * FLOPS_PER_P2P_PAIR / (st["P2P_M2P_L2P"] * 1e-3) / 1e12
+    had = {"bound": "hbm", "achieved": had_bytes / (had_ms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
+           "unit": "GB/s", "frac": None, "traffic": None, "kernel": "k_hadamard (M2L)",
+           "algorithmic_bytes_per_launch": had_bytes, "ms_per_launch": had_ms, "peak_source": src}
+    had["frac"] = had["achieved"] / had["peak"]
+    ev = {"bound": "fp32-simt", "achieved": eval_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+          "frac": eval_tflops / fp32_peak, "kernel": "k_eval (P2P+M2P+L2P)", "pairs_per_launch": pairs,
+          "flops_per_pair": FLOPS_PER_P2P_PAIR, "ms_per_launch": st["P2P_M2P_L2P"],
+          "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 at the sampled SM clock"}
+    return had, ev
+
+
+def cpu_baseline(n_sample, steps=1):
+    """The reference's own OpenMP CPU FMM (oracle/_ref) on a bounded sample of the workload."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    x, q = workload(n_sample)
+    f = ref.RefFmm("laplace", P, NCRIT)
+    t0 = time.perf_counter()
+    f.setup(x, q, x)
+    setup_s = time.perf_counter() - t0
+    f.evaluate()  # warm-up
+    times, stages = [], None
+    for _ in range(steps):
+        f.clear_values()
+        t0 = time.perf_counter()
+        _, stages = f.evaluate(stage_times=True)
+        times.append(time.perf_counter() - t0)
+    f.close()
+    cores = ref.lib().ref_num_threads()
+    t = float(np.median(times))
+    return {"value": n_sample / t / 1e6, "unit": "Mparticles/s", "cores": cores, "kind": "reference",
+            "sample": "N=%d (same p=8, ncrit=128, uniform cube, seeds 0/1), evaluate = upward+downward pass, "
+                      "median of %d after 1 warm-up; tree/lists/precompute excluded (setup %.1fs); FFTW3 served "
+                      "by the oracle's own FFTW-API shim, BLAS/LAPACK by the bundled OpenBLAS"
+                      % (n_sample, steps, setup_s),
+            "stage_s": {k: round(float(v), 4) for k, v in stages.items()}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+        n_sample = min(args.n, 1_000_000)
+        cb = cpu_baseline(n_sample, steps=max(1, min(args.steps, 3)))
+        if cb is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference build missing"}))
+            return
+        line = {"metric": METRIC, "value": cb["value"], "unit": "Mparticles/s", "n_gpus": args.gpus,
+                "steps": max(1, min(args.steps, 3)), "warmup": 1, "ms_per_step": n_sample / cb["value"] / 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": "Laplace FMM evaluate, uniform cube, p=8, ncrit=128", "n_sample": n_sample},
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": "Mparticles/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res, outs, x, q = run_ours(args, rank, world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    acc = accuracy(outs, x, q)
+    peaks, src = measured_peaks()
+    m = res["mixed"]
+    had, ev = roofline(m, peaks, src)
+    n = args.n
+    value = n * world / (m["ms"] * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mparticles/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (P2P, M2L, M2M/L2L) + f64 (pinv, far-field eval)",
+        "data": "synthetic (seeded numpy, uniform cube)",
+        "config": {"workload": "Laplace FMM evaluate (upward+downward), N=%d per GPU, uniform cube, p=8, ncrit=128, "
+                               "adaptive+balanced, sources=targets" % n,
+                   "n_per_gpu": n, "p": P, "ncrit": NCRIT, "l2_flush": "inputs larger than L2 (bodies 256 MB, "
+                                                                           "M2L spectra ~4 GB)",
+                   "tree": m["info"]},
+        "accuracy_vs_fp64_direct_1000_targets": acc,
+        "clocks": m["clocks"],
+        "e2e": {"value": n * world / (m["e2e_ms"] * 1e-3) / 1e6, "unit": "Mparticles/s",
+                "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 4 * 8,
+                "note": "exafmm.laplace.update_charges + evaluate on pinned host arrays (C ABI host path), wall clock incl. copies"},
+        "gpu_launches": int(m["stages"]["launches"]) * args.steps,
+        "roofline": had,
+        "roofline_eval": ev,
+        "stages_ms": {k: round(v, 3) for k, v in m["stages"].items() if k != "launches"},
+        "setup_s": m["setup_s"],
+    }
+    if "fp64" in res:
+        f = res["fp64"]
+        line["fp64_gpu"] = {"value": n * world / (f["ms"] * 1e-3) / 1e6, "ms_per_step": f["ms"],
+                            "stages_ms": {k: round(v, 3) for k, v in f["stages"].items()},
+                            "e2e_value": n * world / (f["e2e_ms"] * 1e-3) / 1e6}
+        line["mixed_over_fp64"] = f["ms"] / m["ms"]
+    if not args.no_cpu_baseline and world == 1:
+        cb = cpu_baseline(min(n, 1_000_000))
+        if cb is not None:
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            line["cpu_baseline"]["stage_s"] = cb["stage_s"]
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

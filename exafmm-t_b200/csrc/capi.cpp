@@ -201,9 +201,9 @@ xfmm_status xfmm_get_values(xfmm_fmm* fmm, xfmm_tree* tree, double* out, int on_
     if (on_device) {
       xfmm::get_values(fmm->f, tree->t, out, S(stream));
     } else {
-      xfmm::DBuf<double> tmp(n);
-      xfmm::get_values(fmm->f, tree->t, tmp.p, S(stream));
-      XCUDA(cudaMemcpyAsync(out, tmp.p, n * sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
+      tree->t.stage_out.reserve(n);
+      xfmm::get_values(fmm->f, tree->t, tree->t.stage_out.p, S(stream));
+      XCUDA(cudaMemcpyAsync(out, tree->t.stage_out.p, n * sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
       XCUDA(cudaStreamSynchronize(S(stream)));
     }
   });
@@ -219,9 +219,9 @@ xfmm_status xfmm_evaluate(xfmm_fmm* fmm, xfmm_tree* tree, double* out, int on_de
     if (on_device) {
       xfmm::get_values(fmm->f, tree->t, out, S(stream));
     } else {
-      xfmm::DBuf<double> tmp(n);
-      xfmm::get_values(fmm->f, tree->t, tmp.p, S(stream));
-      XCUDA(cudaMemcpyAsync(out, tmp.p, n * sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
+      tree->t.stage_out.reserve(n);
+      xfmm::get_values(fmm->f, tree->t, tree->t.stage_out.p, S(stream));
+      XCUDA(cudaMemcpyAsync(out, tree->t.stage_out.p, n * sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
       XCUDA(cudaStreamSynchronize(S(stream)));
     }
   });
@@ -290,10 +290,10 @@ xfmm_status xfmm_tree_dump(const xfmm_tree* tree, double* geo, uint64_t* key, in
   });
 }
 
-xfmm_status xfmm_stage_times(const xfmm_fmm* fmm, double* ms11) {
+xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms12) {
   return guarded([&] {
-    XREQUIRE(fmm && ms11, XFMM_ERR_ARG, "null argument");
-    for (int i = 0; i < 11; i++) ms11[i] = fmm->f.stage_ms[i];
+    XREQUIRE(fmm && tree && ms12, XFMM_ERR_ARG, "null argument");
+    xfmm::stage_times(fmm->f, tree->t, ms12);
   });
 }
 

@@ -91,7 +91,7 @@ struct EvalArgs {
   const void* eq;  // working values [nleafs][nsurf]
   double* out;     // tree order, 4 values per target (complex: interleaved)
   double k_re, k_im;
-  int do_near, do_far, accumulate;
+  int do_near, do_far, accumulate, hilo;
 };
 
 constexpr int EVAL_WARPS = 4;
@@ -106,7 +106,9 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
   const int w = blockIdx.x * EVAL_WARPS + wid;
   if (w >= a.n_eval) return;
   __shared__ V4 s_xyz[EVAL_WARPS][32];
+  __shared__ V4 s_lo[EVAL_WARPS][32];  // FP32: low parts of the leaf-relative coordinates
   __shared__ Q s_q[EVAL_WARPS][32];
+  constexpr bool HILO = sizeof(R) == 4;
   const G g{(R)a.k_re, (R)a.k_im};
   const int pos = a.eval_leafs[w];
   const int node = a.leafs[pos];
@@ -121,12 +123,18 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
     while (G2 * 2 * Tc <= 32) G2 *= 2;
     const int tl = lane / G2, sub = lane % G2;
     const bool active = tl < Tc;
-    R tx = 0, ty = 0, tz = 0;
+    // leaf-relative target coordinates; in FP32 as hi + lo so that differences keep ~FP32
+    // relative accuracy of the separation itself (not of the leaf size)
+    R tx = 0, ty = 0, tz = 0, lx = 0, ly = 0, lz = 0;
     if (active) {
       const double4 t = a.trg4[tb + t0 + tl];
-      tx = (R)(t.x - c.x);
-      ty = (R)(t.y - c.y);
-      tz = (R)(t.z - c.z);
+      const double dx = t.x - c.x, dy = t.y - c.y, dz = t.z - c.z;
+      tx = (R)dx;
+      ty = (R)dy;
+      tz = (R)dz;
+      lx = (R)(dx - (double)tx);
+      ly = (R)(dy - (double)ty);
+      lz = (R)(dz - (double)tz);
     }
     A P, GX, GY, GZ;
     P = GX = GY = GZ = A();
@@ -134,11 +142,20 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
     auto consume = [&](int cnt) {
       __syncwarp();
       Q p = vzero<Q>(), gx = vzero<Q>(), gy = vzero<Q>(), gz = vzero<Q>();
-      if (active)
-        for (int j = sub; j < cnt; j += G2) {
-          const V4 s = s_xyz[wid][j];
-          g.grad(tx - s.x, ty - s.y, tz - s.z, s_q[wid][j], p, gx, gy, gz);
+      if (active) {
+        if (HILO && a.hilo) {
+          for (int j = sub; j < cnt; j += G2) {
+            const V4 s = s_xyz[wid][j], sl = s_lo[wid][j];
+            g.grad((tx - s.x) + (lx - sl.x), (ty - s.y) + (ly - sl.y), (tz - s.z) + (lz - sl.z), s_q[wid][j], p, gx,
+                   gy, gz);
+          }
+        } else {
+          for (int j = sub; j < cnt; j += G2) {
+            const V4 s = s_xyz[wid][j];
+            g.grad(tx - s.x, ty - s.y, tz - s.z, s_q[wid][j], p, gx, gy, gz);
+          }
         }
+      }
       acc64(P, p);
       acc64(GX, gx);
       acc64(GY, gy);
@@ -154,7 +171,10 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
           const int cnt = min(32, ns - j0);
           if (lane < cnt) {
             const double4 sv = a.src4[sb + j0 + lane];
-            s_xyz[wid][lane] = V4{(R)(sv.x - c.x), (R)(sv.y - c.y), (R)(sv.z - c.z), (R)0};
+            const double dx = sv.x - c.x, dy = sv.y - c.y, dz = sv.z - c.z;
+            const R hx = (R)dx, hy = (R)dy, hz = (R)dz;
+            s_xyz[wid][lane] = V4{hx, hy, hz, (R)0};
+            s_lo[wid][lane] = V4{(R)(dx - (double)hx), (R)(dy - (double)hy), (R)(dz - (double)hz), (R)0};
             s_q[wid][lane] = load_charge<Q>(sv, a.src_qim, sb + j0 + lane);
           }
           consume(cnt);
@@ -174,6 +194,7 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
             const int k = j0 + lane;
             s_xyz[wid][lane] = V4{(R)(cs.x + a.surf_base[3 * k] * b - c.x), (R)(cs.y + a.surf_base[3 * k + 1] * b - c.y),
                                   (R)(cs.z + a.surf_base[3 * k + 2] * b - c.z), (R)0};
+            s_lo[wid][lane] = V4{(R)0, (R)0, (R)0, (R)0};
             s_q[wid][lane] = upv[(int64_t)s * n + k];
           }
           consume(cnt);
@@ -187,6 +208,7 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
           const int k = j0 + lane;
           s_xyz[wid][lane] = V4{(R)(a.surf_base[3 * k] * b), (R)(a.surf_base[3 * k + 1] * b),
                                 (R)(a.surf_base[3 * k + 2] * b), (R)0};
+          s_lo[wid][lane] = V4{(R)0, (R)0, (R)0, (R)0};
           s_q[wid][lane] = eqv[(int64_t)pos * n + k];
         }
         consume(cnt);
@@ -494,6 +516,7 @@ struct Workspace {
   DBuf<char> grid, specA, specB;
   std::vector<cufftHandle> fwd, bwd;
   size_t hadamard_smem = 0;
+  int64_t launches = 0;  // kernels of this library launched by the last evaluate
   cudaEvent_t ev[8] = {};
   std::vector<cudaEvent_t> m2l_ev;  // 4 per M2L group
   bool ev_ok = false;
@@ -655,6 +678,7 @@ struct Engine {
 
   static void upward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s) {
     const int n = f.nsurf;
+    ws.launches = 0;
     XCUDA(cudaEventRecord(ws.ev[0], s));
     // P2M: check potentials of every leaf, then the pinv (UC2E) GEMM per leaf level
     if (t.nleafs) {
@@ -662,6 +686,7 @@ struct Engine {
                     t.src4.p,   t.src_qim.p, f.surf_base.p, n,      2.95,      ws.chk.p, 0,         f.k_re, f.k_im};
       k_surf_pot<KER, R><<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
       XLAUNCH();
+      ws.launches++;
       W* up = (W*)ws.up.p;
       for (int l = 0; l <= t.depth; l++) {
         if (KER == K_LAPLACE && l > 0) break;
@@ -670,8 +695,10 @@ struct Engine {
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
         const Ops<W> o = ops_of<W>(f, l);
+        ws.launches++;
         gemm_rows<W>(m, n, n, (const W*)ws.chk.p, ws.p2m1.a.p + off, o.p2m1, (W*)ws.eq.p, ws.p2m1.c.p + off,
                      nullptr, 0, s);
+        ws.launches++;
         gemm_rows<W>(m, n, n, (const W*)ws.eq.p, ws.p2m2.a.p + off, o.p2m2, up, ws.p2m2.c.p + off,
                      alpha_of<R>(ws.p2m2) + off, 0, s);
       }
@@ -680,7 +707,8 @@ struct Engine {
     // M2M: deepest parents first (post-order)
     for (int l = t.depth - 1; l >= 0; l--) {
       const GemmRows& g = ws.m2m[l];
-      gemm_rows<W>(g.M, n, 8 * n, (const W*)ws.up.p, g.a.p, ops_of<W>(f, l).m2m, (W*)ws.up.p, g.c.p, nullptr, 0, s);
+      ws.launches++;
+        gemm_rows<W>(g.M, n, 8 * n, (const W*)ws.up.p, g.a.p, ops_of<W>(f, l).m2m, (W*)ws.up.p, g.c.p, nullptr, 0, s);
     }
     XCUDA(cudaEventRecord(ws.ev[2], s));
   }
@@ -701,7 +729,9 @@ struct Engine {
       k_m2l_grid_up<W><<<std::min<int64_t>(nblk((int64_t)ns * 8 * nconv), 148 * 32), 256, 0, s>>>(
           src, ns, t.child0.p, (const W*)ws.up.p, n, f.conv_to_surf_up.p, nconv, (W*)ws.grid.p);
       XLAUNCH();
+      ws.launches++;
       exec_fwd(ws.fwd[g], ws.grid.p, ws.specA.p);
+      ws.launches++;
       transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, (int64_t)ns * 8, nfreq, s);  // -> [f][s][c]
       XCUDA(cudaEventRecord(ev[1], s));
       // Hadamard product
@@ -715,14 +745,17 @@ struct Engine {
                                                                     t.m2l_tab.p + (int64_t)t.m2l_trg_off[g] * 26, ns,
                                                                     nt, nfreq);
       XLAUNCH();
+      ws.launches++;
       XCUDA(cudaEventRecord(ev[2], s));
       // inverse FFT to downward check potentials (fmm_scale_invariant.h:606-646)
+      ws.launches++;
       transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, nfreq, (int64_t)nt * 8, s);  // -> [t][c][f]
       exec_bwd(ws.bwd[g], ws.specB.p, ws.grid.p);
       k_m2l_gather_dn<W, R><<<std::min<int64_t>(nblk((int64_t)nt * 8 * n), 148 * 32), 256, 0, s>>>(
           trg, nt, t.child0.p, (const W*)ws.grid.p, nconv, f.map_dn.p, n,
           m2l_scale_of<R>(t) + t.m2l_trg_off[g], (W*)ws.dn.p);
       XLAUNCH();
+      ws.launches++;
       XCUDA(cudaEventRecord(ev[3], s));
     }
   }
@@ -755,6 +788,7 @@ struct Engine {
                     f.k_im};
       k_surf_pot<KER, R><<<nblk(t.n_p2l_nodes, 4), 128, 0, s>>>(a);
       XLAUNCH();
+      ws.launches++;
     }
     XCUDA(cudaEventRecord(ws.ev[3], s));
     // M2L
@@ -763,7 +797,8 @@ struct Engine {
     // L2L: shallowest parents first (pre-order)
     for (int l = 0; l < t.depth; l++) {
       const GemmRows& g = ws.l2l[l];
-      gemm_rows<W>(g.M, 8 * n, n, (const W*)ws.dn.p, g.a.p, ops_of<W>(f, l).l2l, (W*)ws.dn.p, g.c.p, nullptr, 1, s);
+      ws.launches++;
+        gemm_rows<W>(g.M, 8 * n, n, (const W*)ws.dn.p, g.a.p, ops_of<W>(f, l).l2l, (W*)ws.dn.p, g.c.p, nullptr, 1, s);
     }
     XCUDA(cudaEventRecord(ws.ev[5], s));
     // L2P part 1: downward check -> equivalent (DC2E) per leaf level
@@ -775,8 +810,10 @@ struct Engine {
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
         const Ops<W> o = ops_of<W>(f, l);
+        ws.launches++;
         gemm_rows<W>(m, n, n, (const W*)ws.dn.p, ws.l2p1.a.p + off, o.l2p1, (W*)ws.chk.p, ws.l2p1.c.p + off,
                      nullptr, 0, s);
+        ws.launches++;
         gemm_rows<W>(m, n, n, (const W*)ws.chk.p, ws.l2p2.a.p + off, o.l2p2, (W*)ws.eq.p, ws.l2p2.c.p + off,
                      alpha_of<R>(ws.l2p2) + off, 0, s);
       }
@@ -787,9 +824,10 @@ struct Engine {
       EvalArgs a{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.level.p,     t.n_eval_leafs, t.sbeg.p,
                  t.tbeg.p,       t.center.p, t.src4.p,   t.trg4.p,  t.src_qim.p,   t.p2p_off.p,    t.m2p_off.p,
                  t.p2p.p,        t.m2p.p,   f.surf_base.p, n,        ws.up.p,       ws.eq.p,        ws.out.p,
-                 f.k_re,         f.k_im,    1,           1,         0};
+                 f.k_re,         f.k_im,    1,           1,         0,             1};
       k_eval<KER, R><<<nblk(t.n_eval_leafs, EVAL_WARPS), 32 * EVAL_WARPS, 0, s>>>(a);
       XLAUNCH();
+      ws.launches++;
     }
     XCUDA(cudaEventRecord(ws.ev[7], s));
   }
@@ -828,10 +866,9 @@ void set_charges(Fmm& f, Tree& t, const double* q, bool on_device, cudaStream_t 
   const int64_t n = t.nsrc;
   const int vs = f.is_complex() ? 2 : 1;
   const double* dq = q;
-  DBuf<double> tmp;
   if (!on_device) {
-    tmp.upload(q, n * vs, s);
-    dq = tmp.p;
+    t.stage_q.upload(q, n * vs, s);  // grow-only staging buffer owned by the tree
+    dq = t.stage_q.p;
   }
   k_set_charges<<<nblk(n), 256, 0, s>>>(dq, t.src_perm.p, n, f.is_complex(), t.src4.p, t.src_qim.p);
   XLAUNCH();
@@ -880,6 +917,7 @@ void stage_times(Fmm& f, Tree& t, double* ms11) {
     ms11[10] += el(e[2], e[3]);
   }
   for (int i = 0; i < 11; i++) f.stage_ms[i] = ms11[i];
+  ms11[11] = (double)ws->launches;
 }
 
 void get_values(Fmm& f, Tree& t, double* out_dev, cudaStream_t s) {
@@ -887,6 +925,7 @@ void get_values(Fmm& f, Tree& t, double* out_dev, cudaStream_t s) {
   const int width = 4 * (f.is_complex() ? 2 : 1);
   k_scatter_out<<<nblk(t.ntrg), 256, 0, s>>>(ws.out.p, t.trg_perm.p, t.ntrg, width, out_dev);
   XLAUNCH();
+  ws.launches++;
 }
 
 // xfmm_gradient_p2p: one "leaf" of all targets against one "leaf" of all sources

@@ -142,6 +142,8 @@ struct Tree {
   DBuf<float> m2l_scale;              // per target 2^(level+1) (Laplace) else 1
   DBuf<double> m2l_scale64;
   int n_m2l_src = 0, n_m2l_trg = 0;
+  // persistent staging for host-side charges and results (no allocation per call)
+  DBuf<double> stage_q, stage_out;
 };
 
 // Precomputed operators of one level (or the single scale-invariant level).
@@ -192,7 +194,7 @@ void clear_values(Fmm& fmm, Tree& t, cudaStream_t s);
 void upward_pass(Fmm& fmm, Tree& t, cudaStream_t s);
 void downward_pass(Fmm& fmm, Tree& t, cudaStream_t s);
 void get_values(Fmm& fmm, Tree& t, double* out_dev, cudaStream_t s);
-void stage_times(Fmm& fmm, Tree& t, double* ms11);
+void stage_times(Fmm& fmm, Tree& t, double* ms12);
 void gradient_p2p_raw(int kernel, double k_re, double k_im, int precision, const double* src, int64_t ns,
                       const double* q, const double* trg, int64_t nt, double* out, cudaStream_t s);
 void verify(Fmm& fmm, Tree& t, int sample, double* err2, cudaStream_t s);

@@ -102,13 +102,13 @@ class FmmBase:
         _lib.check(_lib.lib().xfmm_verify(self._h, tree._h, int(bool(sample)), e.ctypes.data, _current_stream()))
         return [float(e[0]), float(e[1])]
 
-    def stage_times(self):
-        """Device ms of the last evaluate: P2M, M2M, P2L, M2L, L2L, L2P(check->equiv), P2P+M2P+L2P,
-        total, and the M2L FFT / Hadamard / iFFT sub-stages."""
-        t = np.zeros(11)
-        _lib.check(_lib.lib().xfmm_stage_times(self._h, t.ctypes.data))
+    def stage_times(self, tree):
+        """Device ms of the last evaluate on ``tree``: P2M, M2M, P2L, M2L, L2L, L2P(check->equiv),
+        P2P+M2P+L2P, total, and the M2L FFT / Hadamard / iFFT sub-stages."""
+        t = np.zeros(12)
+        _lib.check(_lib.lib().xfmm_stage_times(self._h, tree._h, t.ctypes.data))
         names = ["P2M", "M2M", "P2L", "M2L", "L2L", "L2P_dc2e", "P2P_M2P_L2P", "total", "M2L_fft", "M2L_hadamard",
-                 "M2L_ifft"]
+                 "M2L_ifft", "launches"]
         return dict(zip(names, t.tolist()))
 
     def __del__(self):
@@ -319,7 +319,7 @@ def evaluate(tree, fmm, verbose=False, out=None):
     op, odev = _lib.ptr(out)
     _lib.check(L.xfmm_evaluate(fmm._h, tree._h, op, odev, _current_stream()))
     if verbose:
-        for k, v in fmm.stage_times().items():
+        for k, v in fmm.stage_times(tree).items():
             print("%-20s : %.7e ms" % (k, v))
     return out
 

@@ -105,9 +105,11 @@ xfmm_status xfmm_tree_dump(const xfmm_tree* tree, double* geo, uint64_t* key, in
                            int32_t* nonleafs, int32_t* src_perm, int32_t* trg_perm, int32_t* colleagues,
                            int32_t* m2l, int64_t* p2p_off, int32_t* p2p, int64_t* m2p_off, int32_t* m2p,
                            int64_t* p2l_off, int32_t* p2l);
-/* Per-stage device times (ms) of the last evaluate: P2M, M2M, P2L, M2P+L2P, P2P, M2L, L2L, total;
- * and the M2L sub-stages FFT, Hadamard, iFFT (11 doubles). */
-xfmm_status xfmm_stage_times(const xfmm_fmm* fmm, double* ms11);
+/* Device times (ms, CUDA events) of the last upward + downward pass on this tree: P2M, M2M, P2L,
+ * M2L, L2L, L2P check-to-equivalent, target evaluation (P2P + M2P + L2P), total; then the M2L
+ * sub-stages FFT, Hadamard, iFFT; and the number of this library's kernel launches in the last
+ * evaluate (12 doubles).  Waits for the last pass to finish. */
+xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms12);
 
 /* Direct near-field kernel over raw arrays: out (ntrg x 4) += potential and gradient
  * at trg from (src, q).  precision selects the FP64 or FP32 device kernel. */
