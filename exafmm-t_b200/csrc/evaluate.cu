@@ -51,6 +51,19 @@ template <> __device__ __forceinline__ double2 load_charge<double2>(const double
   return make_double2(s.w, qim[j]);
 }
 
+template <class To> __device__ __forceinline__ To cvt(float v);
+template <class To> __device__ __forceinline__ To cvt(double v);
+template <class To> __device__ __forceinline__ To cvt(float2 v);
+template <class To> __device__ __forceinline__ To cvt(double2 v);
+template <> __device__ __forceinline__ float cvt<float>(float v) { return v; }
+template <> __device__ __forceinline__ float cvt<float>(double v) { return (float)v; }
+template <> __device__ __forceinline__ double cvt<double>(float v) { return (double)v; }
+template <> __device__ __forceinline__ double cvt<double>(double v) { return v; }
+template <> __device__ __forceinline__ float2 cvt<float2>(float2 v) { return v; }
+template <> __device__ __forceinline__ float2 cvt<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <> __device__ __forceinline__ double2 cvt<double2>(float2 v) { return make_double2(v.x, v.y); }
+template <> __device__ __forceinline__ double2 cvt<double2>(double2 v) { return v; }
+
 // FP64 accumulation of FP32/FP64 partials
 __device__ __forceinline__ void acc64(double& a, float b) { a += (double)b; }
 __device__ __forceinline__ void acc64(double& a, double b) { a += b; }
@@ -96,7 +109,9 @@ struct EvalArgs {
 
 constexpr int EVAL_WARPS = 4;
 
-template <int KER, class R>
+// R: arithmetic of the pair interactions; W: value type of the upward equivalent densities (M2P
+// sources).  The downward equivalent densities (L2P sources) are FP64 (the pinv output).
+template <int KER, class R, class W>
 __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
   using G = Green<KER, R>;
   using Q = typename G::Q;
@@ -115,8 +130,9 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
   const int T = a.ntrgs[node];
   const int64_t tb = a.tbeg[node];
   const double4 c = a.center[node];
-  const Q* upv = (const Q*)a.up;
-  const Q* eqv = (const Q*)a.eq;
+  using Q64 = typename Acc64<Q>::type;
+  const W* upv = (const W*)a.up;
+  const Q64* eqv = (const Q64*)a.eq;
   for (int t0 = 0; t0 < T; t0 += 32) {
     const int Tc = min(32, T - t0);
     int G2 = 1;  // lanes per target: source stride
@@ -195,7 +211,7 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
             s_xyz[wid][lane] = V4{(R)(cs.x + a.surf_base[3 * k] * b - c.x), (R)(cs.y + a.surf_base[3 * k + 1] * b - c.y),
                                   (R)(cs.z + a.surf_base[3 * k + 2] * b - c.z), (R)0};
             s_lo[wid][lane] = V4{(R)0, (R)0, (R)0, (R)0};
-            s_q[wid][lane] = upv[(int64_t)s * n + k];
+            s_q[wid][lane] = cvt<Q>(upv[(int64_t)s * n + k]);
           }
           consume(cnt);
         }
@@ -209,7 +225,7 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
           s_xyz[wid][lane] = V4{(R)(a.surf_base[3 * k] * b), (R)(a.surf_base[3 * k + 1] * b),
                                 (R)(a.surf_base[3 * k + 2] * b), (R)0};
           s_lo[wid][lane] = V4{(R)0, (R)0, (R)0, (R)0};
-          s_q[wid][lane] = eqv[(int64_t)pos * n + k];
+          s_q[wid][lane] = cvt<Q>(eqv[(int64_t)pos * n + k]);
         }
         consume(cnt);
       }
@@ -229,6 +245,371 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
       put_out(o + 2 * vs, GY, INV4PI, a.accumulate);
       put_out(o + 3 * vs, GZ, INV4PI, a.accumulate);
     }
+  }
+}
+
+// ================================================================ near field (P2P)
+// Warp per target leaf.  The sources of the leaf's P2P list form one continuous stream that is
+// staged 32 at a time in shared memory as leaf-relative coordinates (FP32: hi + lo parts, so the
+// separation keeps FP32 relative accuracy); only the stream's last chunk is padded (zero charges,
+// far away).  Lanes map to targets in one of two ways:
+//   T >= 32 : TPL targets per lane (t = lane + 32 u), every staged source reused TPL times;
+//   T <  32 : G lanes per target (G = 32 / 2^ceil(log2 T)), each taking every G-th source of a
+//             chunk, partial sums combined with shuffles at the end.
+// FP32 chunk sums are accumulated in FP64.
+struct NearArgs {
+  const int *eval_leafs, *leafs, *nsrcs, *ntrgs;
+  int n_eval;
+  const int64_t *sbeg, *tbeg, *p2p_off;
+  const int* p2p;
+  const double4 *center, *src4, *trg4;
+  const double* src_qim;
+  double* out;
+  double k_re, k_im;
+};
+
+template <class R> struct Stage4;
+template <> struct Stage4<float> { using type = float4; };
+template <> struct Stage4<double> { using type = double4; };
+
+constexpr int NEAR_SEG = 64;  // P2P-list entries held per batch
+
+template <class R>
+struct NearSmem {
+  typename Stage4<R>::type hi[32], lo[32];
+  int64_t seg_beg[NEAR_SEG];
+  int seg_pre[NEAR_SEG + 1];
+};
+
+template <int KER, class R, int TPL>
+__device__ __forceinline__ void near_leaf(const NearArgs& a, int node, int lane, NearSmem<R>& sm) {
+  using G = Green<KER, R>;
+  using Q = typename G::Q;
+  using A = typename Acc64<Q>::type;
+  constexpr bool CPLX = KER == K_HELMHOLTZ;
+  constexpr bool HILO = sizeof(R) == 4;
+  const G g{(R)a.k_re, (R)a.k_im};
+  const int T = a.ntrgs[node];
+  const int64_t tb = a.tbeg[node];
+  const double4 c = a.center[node];
+  const int64_t e0 = a.p2p_off[node], e1 = a.p2p_off[node + 1];
+  // lane -> (target slot, source sub-lane)
+  int G2 = 1;
+  if (TPL == 1)
+    while (G2 * 2 * T <= 32) G2 *= 2;
+  const int tl = lane / G2, sub = lane % G2;
+  const int nper = 32 / G2;  // sources per lane per chunk
+  for (int t0 = 0; t0 < T; t0 += 32 * TPL) {
+    R tx[TPL], ty[TPL], tz[TPL], lx[TPL], ly[TPL], lz[TPL];
+    A P[TPL], GX[TPL], GY[TPL], GZ[TPL];
+#pragma unroll
+    for (int u = 0; u < TPL; u++) {
+      const int t = t0 + tl + 32 * u;
+      double dx = 0, dy = 0, dz = 0;
+      if (t < T) {
+        const double4 v = a.trg4[tb + t];
+        dx = v.x - c.x;
+        dy = v.y - c.y;
+        dz = v.z - c.z;
+      }
+      tx[u] = (R)dx;
+      ty[u] = (R)dy;
+      tz[u] = (R)dz;
+      lx[u] = (R)(dx - (double)tx[u]);
+      ly[u] = (R)(dy - (double)ty[u]);
+      lz[u] = (R)(dz - (double)tz[u]);
+      P[u] = GX[u] = GY[u] = GZ[u] = A();
+    }
+    for (int64_t eb = e0; eb < e1; eb += NEAR_SEG) {
+      // segment table of this batch: begin offsets and an inclusive prefix of counts
+      const int nseg = (int)(e1 - eb < NEAR_SEG ? e1 - eb : NEAR_SEG);
+      __syncwarp();
+      int carry = 0;
+      for (int k0 = 0; k0 < nseg; k0 += 32) {
+        const int k = k0 + lane;
+        int cnt = 0;
+        if (k < nseg) {
+          const int sn = a.p2p[eb + k];
+          cnt = a.nsrcs[sn];
+          sm.seg_beg[k] = a.sbeg[sn];
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        if (k < nseg) sm.seg_pre[k + 1] = carry + incl;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (lane == 0) sm.seg_pre[0] = 0;
+      __syncwarp();
+      const int total = carry;
+      int seg = 0;  // per-lane cursor into the segment table
+      for (int p0 = 0; p0 < total; p0 += 32) {
+        const int pos = p0 + lane;
+        __syncwarp();
+        if (pos < total) {
+          while (sm.seg_pre[seg + 1] <= pos) seg++;
+          const int64_t si = sm.seg_beg[seg] + (pos - sm.seg_pre[seg]);
+          const double4 sv = a.src4[si];
+          const double dx = sv.x - c.x, dy = sv.y - c.y, dz = sv.z - c.z;
+          const R hx = (R)dx, hy = (R)dy, hz = (R)dz;
+          const R qi = CPLX ? (R)a.src_qim[si] : (R)0;
+          sm.hi[lane] = {hx, hy, hz, (R)sv.w};
+          sm.lo[lane] = {(R)(dx - (double)hx), (R)(dy - (double)hy), (R)(dz - (double)hz), qi};
+        } else {
+          sm.hi[lane] = {(R)1e3, (R)1e3, (R)1e3, (R)0};  // zero-charge padding, far from every target
+          sm.lo[lane] = {(R)0, (R)0, (R)0, (R)0};
+        }
+        __syncwarp();
+        Q p[TPL], gx[TPL], gy[TPL], gz[TPL];
+#pragma unroll
+        for (int u = 0; u < TPL; u++) p[u] = gx[u] = gy[u] = gz[u] = vzero<Q>();
+#pragma unroll 4
+        for (int jj = 0; jj < nper; jj++) {
+          const int j = jj * G2 + sub;
+          const auto h = sm.hi[j];
+          const auto l = sm.lo[j];
+          Q q;
+          if constexpr (CPLX) q = Q{h.w, l.w};
+          else q = h.w;
+#pragma unroll
+          for (int u = 0; u < TPL; u++) {
+            R dx, dy, dz;
+            if constexpr (HILO) {
+              dx = (tx[u] - h.x) + (lx[u] - l.x);
+              dy = (ty[u] - h.y) + (ly[u] - l.y);
+              dz = (tz[u] - h.z) + (lz[u] - l.z);
+            } else {
+              dx = tx[u] - h.x;
+              dy = ty[u] - h.y;
+              dz = tz[u] - h.z;
+            }
+            g.grad(dx, dy, dz, q, p[u], gx[u], gy[u], gz[u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < TPL; u++) {
+          acc64(P[u], p[u]);
+          acc64(GX[u], gx[u]);
+          acc64(GY[u], gy[u]);
+          acc64(GZ[u], gz[u]);
+        }
+      }
+    }
+    if (TPL == 1) {
+      for (int o = 1; o < G2; o <<= 1) {
+        P[0] = vadd(P[0], shfl_x(P[0], o));
+        GX[0] = vadd(GX[0], shfl_x(GX[0], o));
+        GY[0] = vadd(GY[0], shfl_x(GY[0], o));
+        GZ[0] = vadd(GZ[0], shfl_x(GZ[0], o));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < TPL; u++) {
+      const int t = t0 + tl + 32 * u;
+      if (t < T && sub == 0) {
+        const int stride = CPLX ? 8 : 4, vs = stride / 4;
+        double* o = a.out + (tb + t) * stride;
+        put_out(o, P[u], INV4PI, 0);
+        put_out(o + vs, GX[u], INV4PI, 0);
+        put_out(o + 2 * vs, GY[u], INV4PI, 0);
+        put_out(o + 3 * vs, GZ[u], INV4PI, 0);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- Laplace FP32 near field, paired FP32
+// Same mapping and streaming as near_leaf, but two sources are processed per instruction with the
+// sm_100 paired FP32 operations (__ffma2_rn / __fadd2_rn / __fmul2_rn): the staged sources are laid
+// out structure-of-arrays so that sources (j, j+1) load as one float2, and the target's coordinates
+// are duplicated into both halves once per chunk.
+struct NearSmemF2 {
+  float hx[32], hy[32], hz[32], q[32], lx[32], ly[32], lz[32];
+  int64_t seg_beg[NEAR_SEG];
+  int seg_pre[NEAR_SEG + 1];
+};
+
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+template <int TPL>
+__device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, int lane, NearSmemF2& sm) {
+  const int T = a.ntrgs[node];
+  const int64_t tb = a.tbeg[node];
+  const double4 c = a.center[node];
+  const int64_t e0 = a.p2p_off[node], e1 = a.p2p_off[node + 1];
+  int G2 = 1;  // at most 16 lanes per target: each lane takes at least one source pair per chunk
+  if (TPL == 1)
+    while (G2 * 2 * T <= 32 && G2 < 16) G2 *= 2;
+  const int tl = lane / G2, sub = lane % G2;
+  const int npl = 16 / G2;  // source pairs per lane per chunk
+  const float2 M1 = make_float2(-1.f, -1.f);
+  for (int t0 = 0; t0 < T; t0 += 32 * TPL) {
+    float2 TX[TPL], TY[TPL], TZ[TPL], LX[TPL], LY[TPL], LZ[TPL];
+    double P[TPL], GX[TPL], GY[TPL], GZ[TPL];
+#pragma unroll
+    for (int u = 0; u < TPL; u++) {
+      const int t = t0 + tl + 32 * u;
+      double dx = 0, dy = 0, dz = 0;
+      if (t < T) {
+        const double4 v = a.trg4[tb + t];
+        dx = v.x - c.x;
+        dy = v.y - c.y;
+        dz = v.z - c.z;
+      }
+      const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
+      TX[u] = dup2(hx);
+      TY[u] = dup2(hy);
+      TZ[u] = dup2(hz);
+      LX[u] = dup2((float)(dx - (double)hx));
+      LY[u] = dup2((float)(dy - (double)hy));
+      LZ[u] = dup2((float)(dz - (double)hz));
+      P[u] = GX[u] = GY[u] = GZ[u] = 0.0;
+    }
+    for (int64_t eb = e0; eb < e1; eb += NEAR_SEG) {
+      const int nseg = (int)(e1 - eb < NEAR_SEG ? e1 - eb : NEAR_SEG);
+      __syncwarp();
+      int carry = 0;
+      for (int k0 = 0; k0 < nseg; k0 += 32) {
+        const int k = k0 + lane;
+        int cnt = 0;
+        if (k < nseg) {
+          const int sn = a.p2p[eb + k];
+          cnt = a.nsrcs[sn];
+          sm.seg_beg[k] = a.sbeg[sn];
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        if (k < nseg) sm.seg_pre[k + 1] = carry + incl;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (lane == 0) sm.seg_pre[0] = 0;
+      __syncwarp();
+      const int total = carry;
+      int seg = 0;
+      for (int p0 = 0; p0 < total; p0 += 32) {
+        const int pos = p0 + lane;
+        __syncwarp();
+        if (pos < total) {
+          while (sm.seg_pre[seg + 1] <= pos) seg++;
+          const double4 sv = a.src4[sm.seg_beg[seg] + (pos - sm.seg_pre[seg])];
+          const double dx = sv.x - c.x, dy = sv.y - c.y, dz = sv.z - c.z;
+          const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
+          sm.hx[lane] = hx;
+          sm.hy[lane] = hy;
+          sm.hz[lane] = hz;
+          sm.q[lane] = (float)sv.w;
+          sm.lx[lane] = (float)(dx - (double)hx);
+          sm.ly[lane] = (float)(dy - (double)hy);
+          sm.lz[lane] = (float)(dz - (double)hz);
+        } else {  // zero-charge padding far from every target
+          sm.hx[lane] = sm.hy[lane] = sm.hz[lane] = 1e3f;
+          sm.q[lane] = sm.lx[lane] = sm.ly[lane] = sm.lz[lane] = 0.f;
+        }
+        __syncwarp();
+        float2 p2[TPL], gx2[TPL], gy2[TPL], gz2[TPL];
+#pragma unroll
+        for (int u = 0; u < TPL; u++) p2[u] = gx2[u] = gy2[u] = gz2[u] = make_float2(0.f, 0.f);
+#pragma unroll 4
+        for (int jj = 0; jj < npl; jj++) {
+          const int j = 2 * (jj * G2 + sub);
+          const float2 HX = *reinterpret_cast<const float2*>(&sm.hx[j]);
+          const float2 HY = *reinterpret_cast<const float2*>(&sm.hy[j]);
+          const float2 HZ = *reinterpret_cast<const float2*>(&sm.hz[j]);
+          const float2 Q = *reinterpret_cast<const float2*>(&sm.q[j]);
+          const float2 SX = *reinterpret_cast<const float2*>(&sm.lx[j]);
+          const float2 SY = *reinterpret_cast<const float2*>(&sm.ly[j]);
+          const float2 SZ = *reinterpret_cast<const float2*>(&sm.lz[j]);
+#pragma unroll
+          for (int u = 0; u < TPL; u++) {
+            // separation (t - s) from hi and lo parts
+            const float2 dx = __fadd2_rn(__ffma2_rn(HX, M1, TX[u]), __ffma2_rn(SX, M1, LX[u]));
+            const float2 dy = __fadd2_rn(__ffma2_rn(HY, M1, TY[u]), __ffma2_rn(SY, M1, LY[u]));
+            const float2 dz = __fadd2_rn(__ffma2_rn(HZ, M1, TZ[u]), __ffma2_rn(SZ, M1, LZ[u]));
+            float2 r2 = __fmul2_rn(dx, dx);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            float ia = rsqrtf(r2.x), ib = rsqrtf(r2.y);
+            ia = r2.x > 0.f ? ia : 0.f;  // r == 0 contributes nothing (laplace.h:57)
+            ib = r2.y > 0.f ? ib : 0.f;
+            const float2 inv = make_float2(ia, ib);
+            const float2 qi = __fmul2_rn(Q, inv);
+            const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
+            p2[u] = __fadd2_rn(p2[u], qi);
+            gx2[u] = __ffma2_rn(qi3, dx, gx2[u]);  // sign applied when accumulating
+            gy2[u] = __ffma2_rn(qi3, dy, gy2[u]);
+            gz2[u] = __ffma2_rn(qi3, dz, gz2[u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < TPL; u++) {
+          P[u] += (double)(p2[u].x + p2[u].y);
+          GX[u] -= (double)(gx2[u].x + gx2[u].y);
+          GY[u] -= (double)(gy2[u].x + gy2[u].y);
+          GZ[u] -= (double)(gz2[u].x + gz2[u].y);
+        }
+      }
+    }
+    if (TPL == 1) {
+      for (int o = 1; o < G2; o <<= 1) {
+        P[0] += __shfl_xor_sync(0xffffffffu, P[0], o);
+        GX[0] += __shfl_xor_sync(0xffffffffu, GX[0], o);
+        GY[0] += __shfl_xor_sync(0xffffffffu, GY[0], o);
+        GZ[0] += __shfl_xor_sync(0xffffffffu, GZ[0], o);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < TPL; u++) {
+      const int t = t0 + tl + 32 * u;
+      if (t < T && sub == 0) {
+        double* o = a.out + (tb + t) * 4;
+        o[0] = P[u] * INV4PI;
+        o[1] = GX[u] * INV4PI;
+        o[2] = GY[u] * INV4PI;
+        o[3] = GZ[u] * INV4PI;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_near_lap_f2(NearArgs a) {
+  __shared__ NearSmemF2 sm[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int w = blockIdx.x * 4 + wid;
+  if (w >= a.n_eval) return;
+  const int node = a.leafs[a.eval_leafs[w]];
+  if (a.ntrgs[node] <= 32) near_leaf_lap_f2<1>(a, node, lane, sm[wid]);
+  else near_leaf_lap_f2<2>(a, node, lane, sm[wid]);
+}
+
+#ifndef XFMM_NEAR_MAXTPL
+#define XFMM_NEAR_MAXTPL 2  // targets per lane of the FP32 near-field kernel (compile-time tunable)
+#endif
+#ifndef XFMM_NEAR_MINB
+#define XFMM_NEAR_MINB 1  // minimum resident blocks per SM requested from the register allocator
+#endif
+
+template <int KER, class R>
+__global__ void __launch_bounds__(128, XFMM_NEAR_MINB) k_near(NearArgs a) {
+  __shared__ NearSmem<R> sm[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int w = blockIdx.x * 4 + wid;
+  if (w >= a.n_eval) return;
+  const int node = a.leafs[a.eval_leafs[w]];
+  const int T = a.ntrgs[node];
+  if constexpr (sizeof(R) == 4) {
+    if (T <= 32 || XFMM_NEAR_MAXTPL == 1) near_leaf<KER, R, 1>(a, node, lane, sm[wid]);
+    else if (T <= 64 || XFMM_NEAR_MAXTPL == 2) near_leaf<KER, R, (XFMM_NEAR_MAXTPL >= 2 ? 2 : 1)>(a, node, lane, sm[wid]);
+    else if (T <= 96 || XFMM_NEAR_MAXTPL == 3) near_leaf<KER, R, (XFMM_NEAR_MAXTPL >= 3 ? 3 : 1)>(a, node, lane, sm[wid]);
+    else near_leaf<KER, R, (XFMM_NEAR_MAXTPL >= 4 ? 4 : 1)>(a, node, lane, sm[wid]);
+  } else {
+    near_leaf<KER, R, 1>(a, node, lane, sm[wid]);  // FP64: one target per lane keeps occupancy up
   }
 }
 
@@ -299,40 +680,41 @@ __global__ void __launch_bounds__(128) k_surf_pot(SurfPotArgs a) {
 
 // ================================================================ translation GEMMs
 // C[coff[i] + j] (+)= alpha[i] * sum_k A[aoff[i] + k] * B[k*N + j]   (rows gathered/scattered)
-template <class V, int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_gemm_rows(int M, int N, int K, const V* __restrict__ A,
+// computed in B's precision; A is converted on load and C on store.
+template <class TA, class TB, class TC, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_gemm_rows(int M, int N, int K, const TA* __restrict__ A,
                                                                       const int64_t* __restrict__ aoff,
-                                                                      const V* __restrict__ B, V* __restrict__ C,
+                                                                      const TB* __restrict__ B, TC* __restrict__ C,
                                                                       const int64_t* __restrict__ coff,
-                                                                      const typename Base<V>::type* __restrict__ alpha,
+                                                                      const typename Base<TB>::type* __restrict__ alpha,
                                                                       int accumulate) {
-  using RB = typename Base<V>::type;
+  using RB = typename Base<TB>::type;
   constexpr int NT = (BM / TM) * (BN / TN);
-  __shared__ V As[BK][BM];
-  __shared__ V Bs[BK][BN];
+  __shared__ TB As[BK][BM];
+  __shared__ TB Bs[BK][BN];
   const int tid = threadIdx.x;
   const int tx = tid % (BN / TN), ty = tid / (BN / TN);
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  V acc[TM][TN];
+  TB acc[TM][TN];
 #pragma unroll
   for (int i = 0; i < TM; i++)
 #pragma unroll
-    for (int j = 0; j < TN; j++) acc[i][j] = vzero<V>();
+    for (int j = 0; j < TN; j++) acc[i][j] = vzero<TB>();
   for (int k0 = 0; k0 < K; k0 += BK) {
     for (int e = tid; e < BM * BK; e += NT) {
       const int r = e / BK, kk = e % BK;
       const int row = m0 + r, k = k0 + kk;
-      As[kk][r] = (row < M && k < K) ? A[aoff[row] + k] : vzero<V>();
+      As[kk][r] = (row < M && k < K) ? cvt<TB>(A[aoff[row] + k]) : vzero<TB>();
     }
     for (int e = tid; e < BK * BN; e += NT) {
       const int kk = e / BN, cc = e % BN;
       const int k = k0 + kk, col = n0 + cc;
-      Bs[kk][cc] = (k < K && col < N) ? B[(int64_t)k * N + col] : vzero<V>();
+      Bs[kk][cc] = (k < K && col < N) ? B[(int64_t)k * N + col] : vzero<TB>();
     }
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < BK; kk++) {
-      V av[TM], bv[TN];
+      TB av[TM], bv[TN];
 #pragma unroll
       for (int i = 0; i < TM; i++) av[i] = As[kk][ty * TM + i];
 #pragma unroll
@@ -349,29 +731,29 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_gemm_rows(int M, int 
     const int row = m0 + ty * TM + i;
     if (row >= M) continue;
     const RB al = alpha ? alpha[row] : RB(1);
-    V* crow = C + coff[row];
+    TC* crow = C + coff[row];
 #pragma unroll
     for (int j = 0; j < TN; j++) {
       const int col = n0 + tx * TN + j;
       if (col < N) {
-        const V v = vscale(acc[i][j], al);
-        crow[col] = accumulate ? vadd(crow[col], v) : v;
+        const TB v = vscale(acc[i][j], al);
+        crow[col] = accumulate ? cvt<TC>(vadd(cvt<TB>(crow[col]), v)) : cvt<TC>(v);
       }
     }
   }
 }
 
-template <class V>
-void gemm_rows(int M, int N, int K, const V* A, const int64_t* aoff, const V* B, V* C, const int64_t* coff,
-               const typename Base<V>::type* alpha, int accumulate, cudaStream_t s) {
+template <class TA, class TB, class TC>
+void gemm_rows(int M, int N, int K, const TA* A, const int64_t* aoff, const TB* B, TC* C, const int64_t* coff,
+               const typename Base<TB>::type* alpha, int accumulate, cudaStream_t s) {
   if (M <= 0) return;
-  constexpr bool cplx = sizeof(V) == 2 * sizeof(typename Base<V>::type);
-  if (cplx) {
+  constexpr bool cplx = sizeof(TB) == 2 * sizeof(typename Base<TB>::type);
+  if constexpr (cplx) {
     dim3 grid((N + 63) / 64, (M + 31) / 32);
-    k_gemm_rows<V, 32, 64, 8, 2, 4><<<grid, 256, 0, s>>>(M, N, K, A, aoff, B, C, coff, alpha, accumulate);
+    k_gemm_rows<TA, TB, TC, 32, 64, 8, 2, 4><<<grid, 256, 0, s>>>(M, N, K, A, aoff, B, C, coff, alpha, accumulate);
   } else {
     dim3 grid((N + 63) / 64, (M + 63) / 64);
-    k_gemm_rows<V, 64, 64, 16, 4, 4><<<grid, 256, 0, s>>>(M, N, K, A, aoff, B, C, coff, alpha, accumulate);
+    k_gemm_rows<TA, TB, TC, 64, 64, 16, 4, 4><<<grid, 256, 0, s>>>(M, N, K, A, aoff, B, C, coff, alpha, accumulate);
   }
   XLAUNCH();
 }
@@ -417,43 +799,235 @@ void transpose(const CT* in, CT* out, int64_t R, int64_t C, cudaStream_t s) {
 
 // Hadamard product per frequency (fmm_scale_invariant.h:343-399; intrinsics.h matmult_8x8x2):
 //   out[f][t][tc] = sum_ipos sum_sc T[ipos][f][sc*8 + tc] * in[f][src(t, ipos)][sc]
-template <class CT, int KC>
-__global__ void __launch_bounds__(256) k_hadamard(const CT* __restrict__ T, const CT* __restrict__ in,
-                                                   CT* __restrict__ out, const int* __restrict__ tab, int nsrc,
-                                                   int ntrg, int nfreq) {
-  extern __shared__ unsigned char smem_raw[];
-  CT* sT = (CT*)smem_raw;  // [26][KC][64]
-  const int f0 = blockIdx.x * KC;
-  for (int e = threadIdx.x; e < 26 * KC * 64; e += blockDim.x) {
-    const int j = e % 64, kk = (e / 64) % KC, ipos = e / (64 * KC);
-    const int f = f0 + kk;
-    sT[e] = f < nfreq ? T[((int64_t)ipos * nfreq + f) * 64 + j] : vzero<CT>();
+// FP64 form: a CTA owns a tile of HAD_TT targets and HAD_KC frequencies.  Each warp owns 32 of the
+// tile's targets at one frequency and streams their (target, source, relative position) pairs in
+// rounds of 32 lanes; rounds are built on the host so that no target occurs twice in a round, hence
+// the shared-memory accumulators need no atomics and no block barrier between positions (the sums
+// are taken in a fixed order), and each lane prefetches its next round while computing the current
+// one.  The FP32 form is k_hadamard_r below.
+constexpr int HAD_TT = 128;  // targets per CTA (4 warps x 32)
+constexpr int HAD_ST = 9;    // accumulator row stride (values): conflict-free for consecutive targets
+
+template <class CT> struct HadKC;
+template <> struct HadKC<double2> { static constexpr int KC = 1; };
+
+__device__ __forceinline__ void had_mac8(const double2* __restrict__ M, const double2* v, double2* o) {
+#pragma unroll
+  for (int sc = 0; sc < 8; sc++)
+#pragma unroll
+    for (int tc = 0; tc < 8; tc++) vfma(o[tc], M[sc * 8 + tc], v[sc]);
+}
+
+template <class CT> struct HadM { using type = CT; };
+
+template <class CT>
+__device__ __forceinline__ void had_load8(const CT* __restrict__ p, CT* v) {
+#pragma unroll
+  for (int i = 0; i < 8; i++) v[i] = p[i];
+}
+template <>
+__device__ __forceinline__ void had_load8<float2>(const float2* __restrict__ p, float2* v) {
+  const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const float4 w = __ldg(q + i);
+    v[2 * i] = make_float2(w.x, w.y);
+    v[2 * i + 1] = make_float2(w.z, w.w);
+  }
+}
+
+template <class CT>
+__global__ void __launch_bounds__(128 * HadKC<CT>::KC) k_hadamard(const CT* __restrict__ T, const CT* __restrict__ in,
+                                                                   CT* __restrict__ out,
+                                                                   const int* __restrict__ grp_off,
+                                                                   const int2* __restrict__ ent, int nsrc, int ntrg,
+                                                                   int nfreq) {
+  constexpr int KC = HadKC<CT>::KC;
+  using MT = typename HadM<CT>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  MT* sM = reinterpret_cast<MT*>(smem_raw);                  // [KC][26][64]
+  CT* sAcc = reinterpret_cast<CT*>(sM + KC * 26 * 64);        // [KC][HAD_TT][HAD_ST]
+  const int tile = blockIdx.x, f0 = blockIdx.y * KC, tid = threadIdx.x;
+  const int lane = tid & 31, wid = tid >> 5;
+  const int kk = wid >> 2, grp = wid & 3;
+  const int t0 = tile * HAD_TT, nt = min(HAD_TT, ntrg - t0);
+  for (int e = tid; e < KC * 26 * 64; e += blockDim.x) {
+    const int j = e & 63, ipos = (e >> 6) % 26, k = e / (26 * 64);
+    const int f = min(f0 + k, nfreq - 1);
+    const CT m = T[((int64_t)ipos * nfreq + f) * 64 + j];
+    sM[e] = m;
+  }
+  for (int e = tid; e < KC * HAD_TT * HAD_ST; e += blockDim.x) sAcc[e] = vzero<CT>();
+  __syncthreads();
+  const int f = f0 + kk;
+  if (f < nfreq) {
+    const CT* inf = in + (int64_t)f * nsrc * 8;
+    const MT* Mk = sM + kk * 26 * 64;
+    CT* acc = sAcc + kk * HAD_TT * HAD_ST;
+    const int e0 = grp_off[tile * 4 + grp], e1 = grp_off[tile * 4 + grp + 1];
+    int2 cur = e0 + lane < e1 ? ent[e0 + lane] : make_int2(-1, 0);
+    CT v[8];
+    if (cur.x >= 0) had_load8<CT>(inf + (int64_t)cur.x * 8, v);
+    for (int e = e0; e < e1; e += 32) {
+      // prefetch the next round
+      int2 nxt = e + 32 + lane < e1 ? ent[e + 32 + lane] : make_int2(-1, 0);
+      CT w[8];
+      if (nxt.x >= 0) had_load8<CT>(inf + (int64_t)nxt.x * 8, w);
+      if (cur.x >= 0) {
+        const int ipos = cur.y >> 8, lt = cur.y & 255;
+        CT o[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) o[i] = vzero<CT>();
+        had_mac8(Mk + ipos * 64, v, o);
+        CT* q = acc + lt * HAD_ST;
+#pragma unroll
+        for (int i = 0; i < 8; i++) q[i] = vadd(q[i], o[i]);
+      }
+      __syncwarp();
+      cur = nxt;
+#pragma unroll
+      for (int i = 0; i < 8; i++) v[i] = w[i];
+    }
   }
   __syncthreads();
-  for (int kk = 0; kk < KC; kk++) {
-    const int f = f0 + kk;
-    if (f >= nfreq) break;
-    const CT* inf = in + (int64_t)f * nsrc * 8;
-    for (int t = threadIdx.x; t < ntrg; t += blockDim.x) {
-      CT acc[8];
+  for (int k = 0; k < KC; k++) {
+    const int ff = f0 + k;
+    if (ff >= nfreq) break;
+    CT* of = out + ((int64_t)ff * ntrg + t0) * 8;
+    const CT* acc = sAcc + k * HAD_TT * HAD_ST;
+    for (int e = tid; e < nt * 8; e += blockDim.x) of[e] = acc[(e >> 3) * HAD_ST + (e & 7)];
+  }
+}
+
+// Hadamard product, round form (FP32 working precision).  The same product as k_hadamard, scheduled
+// for targets with few interactions: a CTA owns HADR_TT targets at one frequency; the tile's pairs are
+// grouped by relative position and packed on the host into rounds of HADR_RW pairs that share one
+// position, so a warp reads the 8x8 block of that position once (a shared-memory broadcast) for the
+// two pairs each lane holds.  Any warp may take any round; targets repeat across concurrent rounds of
+// different positions, so the accumulators are updated with shared-memory atomics (the FP32 sums are
+// therefore taken in a run-dependent order).  Two FP32 operations per instruction (__ffma2_rn), with
+// the 8x8 blocks expanded in shared memory to {re, re, -im, im}.
+#ifndef XFMM_HADR_PREFETCH
+#define XFMM_HADR_PREFETCH 1
+#endif
+constexpr int HADR_NT = 256;            // threads per CTA
+constexpr int HADR_TT = 1024;           // targets per tile
+constexpr int HADR_RST = 17;            // accumulator stride per target in reals (16 values + 1 pad)
+constexpr int HADR_PPL = 2;             // pairs per lane per round
+constexpr int HADR_RW = 32 * HADR_PPL;  // pairs per round
+
+__device__ __forceinline__ void had_mac8x2(const float4* __restrict__ M, const float2* v0, const float2* v1,
+                                           float2* o0, float2* o1) {
 #pragma unroll
-      for (int i = 0; i < 8; i++) acc[i] = vzero<CT>();
-      for (int ipos = 0; ipos < 26; ipos++) {
-        const int s = tab[t * 26 + ipos];
-        if (s < 0) continue;
-        CT v[8];
+  for (int sc = 0; sc < 8; sc++) {
+    const float2 a0 = v0[sc], b0 = make_float2(v0[sc].y, v0[sc].x);
+    const float2 a1 = v1[sc], b1 = make_float2(v1[sc].y, v1[sc].x);
 #pragma unroll
-        for (int i = 0; i < 8; i++) v[i] = inf[(int64_t)s * 8 + i];
-        const CT* M = sT + (ipos * KC + kk) * 64;
-#pragma unroll
-        for (int sc = 0; sc < 8; sc++)
-#pragma unroll
-          for (int tc = 0; tc < 8; tc++) vfma(acc[tc], M[sc * 8 + tc], v[sc]);
-      }
-      CT* o = out + ((int64_t)f * ntrg + t) * 8;
-#pragma unroll
-      for (int i = 0; i < 8; i++) o[i] = acc[i];
+    for (int tc = 0; tc < 8; tc++) {
+      const float4 m = M[sc * 8 + tc];  // {re, re, -im, im}
+      const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
+      o0[tc] = __ffma2_rn(mr, a0, o0[tc]);
+      o1[tc] = __ffma2_rn(mr, a1, o1[tc]);
+      o0[tc] = __ffma2_rn(mi, b0, o0[tc]);
+      o1[tc] = __ffma2_rn(mi, b1, o1[tc]);
     }
+  }
+}
+
+__global__ void __launch_bounds__(HADR_NT, 2) k_hadamard_r(const float2* __restrict__ T, const float2* __restrict__ in,
+                                                           float2* __restrict__ out, const int* __restrict__ tile_r,
+                                                           const int* __restrict__ rpos, const int2* __restrict__ ent,
+                                                           int nsrc, int ntrg, int nfreq) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sM = reinterpret_cast<float4*>(smem_raw);           // [26][64]
+  float* sAcc = reinterpret_cast<float*>(sM + 26 * 64);      // [HADR_TT][HADR_RST]
+  constexpr int NW = HADR_NT / 32;
+  const int tile = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
+  const int lane = tid & 31, wid = tid >> 5;
+  const int t0 = tile * HADR_TT, nt = min(HADR_TT, ntrg - t0);
+  for (int e = tid; e < 26 * 64; e += HADR_NT) {
+    const int j = e & 63, ipos = e >> 6;
+    const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + j];
+    sM[e] = make_float4(m.x, m.x, -m.y, m.y);
+  }
+  for (int e = tid; e < nt * HADR_RST; e += HADR_NT) sAcc[e] = 0.f;
+  __syncthreads();
+  const float2* inf = in + (int64_t)f * nsrc * 8;
+  const int r1 = tile_r[tile + 1];
+  int r = tile_r[tile] + wid;
+  int2 c0 = make_int2(-1, 0), c1 = make_int2(-1, 0);
+  int cpos = 0;
+  float2 v0[8], v1[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) v0[i] = v1[i] = make_float2(0.f, 0.f);
+  if (r < r1) {
+    cpos = rpos[r];
+    c0 = ent[(int64_t)r * HADR_RW + lane];
+    c1 = ent[(int64_t)r * HADR_RW + 32 + lane];
+#if XFMM_HADR_PREFETCH
+    if (c0.x >= 0) had_load8<float2>(inf + (int64_t)c0.x * 8, v0);
+    if (c1.x >= 0) had_load8<float2>(inf + (int64_t)c1.x * 8, v1);
+#endif
+  }
+  for (; r < r1; r += NW) {
+    // prefetch this warp's next round (its pairs, and with XFMM_HADR_PREFETCH their inputs) while
+    // computing the current one
+    const int rn = r + NW;
+    int2 n0 = make_int2(-1, 0), n1 = make_int2(-1, 0);
+    int npos = 0;
+#if XFMM_HADR_PREFETCH
+    float2 w0[8], w1[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w0[i] = w1[i] = make_float2(0.f, 0.f);
+#else
+    if (c0.x >= 0) had_load8<float2>(inf + (int64_t)c0.x * 8, v0);
+    if (c1.x >= 0) had_load8<float2>(inf + (int64_t)c1.x * 8, v1);
+#endif
+    if (rn < r1) {
+      npos = rpos[rn];
+      n0 = ent[(int64_t)rn * HADR_RW + lane];
+      n1 = ent[(int64_t)rn * HADR_RW + 32 + lane];
+#if XFMM_HADR_PREFETCH
+      if (n0.x >= 0) had_load8<float2>(inf + (int64_t)n0.x * 8, w0);
+      if (n1.x >= 0) had_load8<float2>(inf + (int64_t)n1.x * 8, w1);
+#endif
+    }
+    float2 o0[8], o1[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) o0[i] = o1[i] = make_float2(0.f, 0.f);
+    had_mac8x2(sM + cpos * 64, v0, v1, o0, o1);
+    if (c0.x >= 0) {
+      float* q = sAcc + c0.y * HADR_RST;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        atomicAdd(q + 2 * i, o0[i].x);
+        atomicAdd(q + 2 * i + 1, o0[i].y);
+      }
+    }
+    if (c1.x >= 0) {
+      float* q = sAcc + c1.y * HADR_RST;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        atomicAdd(q + 2 * i, o1[i].x);
+        atomicAdd(q + 2 * i + 1, o1[i].y);
+      }
+    }
+    c0 = n0;
+    c1 = n1;
+    cpos = npos;
+#if XFMM_HADR_PREFETCH
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      v0[i] = w0[i];
+      v1[i] = w1[i];
+    }
+#endif
+  }
+  __syncthreads();
+  float2* of = out + ((int64_t)f * ntrg + t0) * 8;
+  for (int e = tid; e < nt * 8; e += HADR_NT) {
+    const float* a = sAcc + (e >> 3) * HADR_RST + 2 * (e & 7);
+    of[e] = make_float2(a[0], a[1]);
   }
 }
 
@@ -506,7 +1080,8 @@ struct GemmRows {
 struct Workspace {
   int precision = -1, kernel = -1, p = 0;
   size_t vsz = 0;
-  DBuf<char> up, dn, chk, eq;
+  DBuf<char> up, dn, chk;  // working precision
+  DBuf<char> ybuf, eq;     // FP64: pinv intermediate, downward equivalent densities of the leaves
   DBuf<double> out;
   // leaves grouped by level (P2M / L2P operators are per level except for Laplace)
   std::vector<int> leaf_level_off;
@@ -515,6 +1090,13 @@ struct Workspace {
   // M2L
   DBuf<char> grid, specA, specB;
   std::vector<cufftHandle> fwd, bwd;
+  // Hadamard tiling: per group, tiles of TT targets; CSR over (tile, ipos) of (local target, source)
+  DBuf<int> had_off;
+  DBuf<int2> had_pairs;
+  std::vector<int> had_tile0;  // first tile of each group (ngroups + 1)
+  // round form (FP32): per tile the range of rounds; per round its relative position and HADR_RW pairs
+  DBuf<int> hadr_tile, hadr_pos;
+  DBuf<int2> hadr_ent;
   size_t hadamard_smem = 0;
   int64_t launches = 0;  // kernels of this library launched by the last evaluate
   cudaEvent_t ev[8] = {};
@@ -565,7 +1147,8 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   W.up.alloc((size_t)t.nnodes * n * W.vsz);
   W.dn.alloc((size_t)t.nnodes * n * W.vsz);
   W.chk.alloc((size_t)std::max(t.nleafs, 1) * n * W.vsz);
-  W.eq.alloc((size_t)std::max(t.nleafs, 1) * n * W.vsz);
+  W.ybuf.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
+  W.eq.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
   W.out.alloc((size_t)t.ntrg * 4 * (cplx ? 2 : 1));
   // leaf rows grouped by level: P2M (chk[pos] -> up[node]) and L2P (dn[node] -> eq[pos])
   const bool lap = f.kernel == XFMM_LAPLACE;
@@ -643,6 +1226,86 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
     W.fwd.push_back(hf);
     W.bwd.push_back(hb);
   }
+  if (f.mixed()) {
+    // round form: per group, tiles of HADR_TT targets; per tile and relative position the pairs
+    // (source index, target index within the tile) in rounds of HADR_RW, padded with source -1.
+    std::vector<int> tile_r, pos;
+    std::vector<int2> ent;
+    W.had_tile0.assign(ng + 1, 0);
+    int ntiles = 0;
+    for (int g = 0; g < ng; g++) {
+      W.had_tile0[g] = ntiles;
+      const int tb = t.m2l_trg_off[g], te = t.m2l_trg_off[g + 1];
+      for (int t0 = tb; t0 < te; t0 += HADR_TT, ntiles++) {
+        tile_r.push_back((int)pos.size());
+        const int t1 = std::min(te, t0 + HADR_TT);
+        for (int ipos = 0; ipos < 26; ipos++) {
+          int k = 0;
+          for (int tt = t0; tt < t1; tt++) {
+            const int sidx = t.h_m2l_tab[26 * (size_t)tt + ipos];
+            if (sidx < 0) continue;
+            if (k == 0) {
+              pos.push_back(ipos);
+              ent.resize(ent.size() + HADR_RW, make_int2(-1, 0));
+            }
+            ent[ent.size() - HADR_RW + k] = make_int2(sidx, tt - t0);
+            if (++k == HADR_RW) k = 0;
+          }
+        }
+      }
+    }
+    W.had_tile0[ng] = ntiles;
+    tile_r.push_back((int)pos.size());
+    if (ent.empty()) {
+      pos.push_back(0);
+      ent.resize(HADR_RW, make_int2(-1, 0));
+    }
+    W.hadr_tile.upload(tile_r, s);
+    W.hadr_pos.upload(pos, s);
+    W.hadr_ent.upload(ent, s);
+  } else {
+    // per group of M2L targets: tiles of HAD_TT targets, 4 warp groups of 32 targets; each warp group's
+    // pairs (ordered by relative position) packed into rounds of 32 lanes with no repeated target,
+    // padded with src = -1.  Entry: {source index, (ipos << 8) | target index within the tile}.
+    std::vector<int> off;
+    std::vector<int2> ent;
+    W.had_tile0.assign(ng + 1, 0);
+    int ntiles = 0;
+    for (int g = 0; g < ng; g++) {
+      W.had_tile0[g] = ntiles;
+      const int tb = t.m2l_trg_off[g], te = t.m2l_trg_off[g + 1];
+      for (int t0 = tb; t0 < te; t0 += HAD_TT, ntiles++) {
+        for (int wg = 0; wg < 4; wg++) {
+          off.push_back((int)ent.size());
+          const int a0 = t0 + 32 * wg, a1 = std::min(te, a0 + 32);
+          std::vector<int2> round;
+          uint64_t used = 0;
+          auto flush = [&]() {
+            if (round.empty()) return;
+            for (auto& r : round) ent.push_back(r);
+            for (size_t k = round.size(); k < 32; k++) ent.push_back(make_int2(-1, 0));
+            round.clear();
+            used = 0;
+          };
+          for (int ipos = 0; ipos < 26; ipos++)
+            for (int tt = a0; tt < a1; tt++) {
+              const int sidx = t.h_m2l_tab[26 * (size_t)tt + ipos];
+              if (sidx < 0) continue;
+              const int lw = tt - a0;
+              if ((used >> lw) & 1 || round.size() == 32) flush();
+              round.push_back(make_int2(sidx, (ipos << 8) | (tt - t0)));
+              used |= (uint64_t)1 << lw;
+            }
+          flush();
+        }
+      }
+    }
+    W.had_tile0[ng] = ntiles;
+    off.push_back((int)ent.size());
+    if (ent.empty()) ent.push_back(make_int2(-1, 0));
+    W.had_off.upload(off, s);
+    W.had_pairs.upload(ent, s);
+  }
   for (auto& e : W.ev) XCUDA(cudaEventCreate(&e));
   W.m2l_ev.resize(4 * (size_t)ng);
   for (auto& e : W.m2l_ev) XCUDA(cudaEventCreate(&e));
@@ -651,19 +1314,19 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   return W;
 }
 
-template <class W>
+template <class W, class V64>
 struct Ops {
-  const W *p2m1, *p2m2, *l2p1, *l2p2, *m2m, *l2l;
+  const V64 *p2m1, *p2m2, *l2p1, *l2p2;  // FP64 check-to-equivalent factors
+  const W *m2m, *l2l;                   // working precision
 };
-template <class W>
-Ops<W> ops_of(const Fmm& f, int level) {
+template <class W, class V64>
+Ops<W, V64> ops_of(const Fmm& f, int level) {
   const LevelOps& o = f.ops[f.kernel == XFMM_LAPLACE ? 0 : level];
-  return Ops<W>{(const W*)o.p2m_B1.p, (const W*)o.p2m_B2.p, (const W*)o.l2p_B1.p, (const W*)o.l2p_B2.p,
-                (const W*)o.m2m_B.p,  (const W*)o.l2l_B.p};
+  return Ops<W, V64>{(const V64*)o.p2m_B1.p, (const V64*)o.p2m_B2.p, (const V64*)o.l2p_B1.p,
+                     (const V64*)o.l2p_B2.p, (const W*)o.m2m_B.p,     (const W*)o.l2l_B.p};
 }
 
 template <class RB> const RB* alpha_of(const GemmRows& g);
-template <> const float* alpha_of<float>(const GemmRows& g) { return g.al32.p; }
 template <> const double* alpha_of<double>(const GemmRows& g) { return g.al64.p; }
 
 template <class RB> const RB* m2l_scale_of(const Tree& t);
@@ -673,8 +1336,9 @@ template <> const double* m2l_scale_of<double>(const Tree& t) { return t.m2l_sca
 // ------------------------------------------------------------------ engine, per kernel and precision
 template <int KER, class R>
 struct Engine {
-  using W = typename Green<KER, R>::Q;  // working value: R or complex
-  using CT = typename C2<R>::type;      // spectrum value
+  using W = typename Green<KER, R>::Q;          // working value: R or complex
+  using V64 = typename Green<KER, double>::Q;   // FP64 value (pinv GEMMs, downward equivalent densities)
+  using CT = typename C2<R>::type;              // spectrum value
 
   static void upward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s) {
     const int n = f.nsurf;
@@ -694,13 +1358,13 @@ struct Engine {
         const int m = KER == K_LAPLACE ? ws.p2m1.M : r1 - r0;
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
-        const Ops<W> o = ops_of<W>(f, l);
+        const Ops<W, V64> o = ops_of<W, V64>(f, l);
         ws.launches++;
-        gemm_rows<W>(m, n, n, (const W*)ws.chk.p, ws.p2m1.a.p + off, o.p2m1, (W*)ws.eq.p, ws.p2m1.c.p + off,
-                     nullptr, 0, s);
+        gemm_rows<W, V64, V64>(m, n, n, (const W*)ws.chk.p, ws.p2m1.a.p + off, o.p2m1, (V64*)ws.ybuf.p,
+                               ws.p2m1.c.p + off, nullptr, 0, s);
         ws.launches++;
-        gemm_rows<W>(m, n, n, (const W*)ws.eq.p, ws.p2m2.a.p + off, o.p2m2, up, ws.p2m2.c.p + off,
-                     alpha_of<R>(ws.p2m2) + off, 0, s);
+        gemm_rows<V64, V64, W>(m, n, n, (const V64*)ws.ybuf.p, ws.p2m2.a.p + off, o.p2m2, up, ws.p2m2.c.p + off,
+                               alpha_of<double>(ws.p2m2) + off, 0, s);
       }
     }
     XCUDA(cudaEventRecord(ws.ev[1], s));
@@ -708,7 +1372,8 @@ struct Engine {
     for (int l = t.depth - 1; l >= 0; l--) {
       const GemmRows& g = ws.m2m[l];
       ws.launches++;
-        gemm_rows<W>(g.M, n, 8 * n, (const W*)ws.up.p, g.a.p, ops_of<W>(f, l).m2m, (W*)ws.up.p, g.c.p, nullptr, 0, s);
+        gemm_rows<W, W, W>(g.M, n, 8 * n, (const W*)ws.up.p, g.a.p, ops_of<W, V64>(f, l).m2m, (W*)ws.up.p, g.c.p,
+                           nullptr, 0, s);
     }
     XCUDA(cudaEventRecord(ws.ev[2], s));
   }
@@ -735,15 +1400,29 @@ struct Engine {
       transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, (int64_t)ns * 8, nfreq, s);  // -> [f][s][c]
       XCUDA(cudaEventRecord(ev[1], s));
       // Hadamard product
-      constexpr int KC = sizeof(R) == 4 ? 4 : 2;
-      const size_t smem = (size_t)26 * KC * 64 * sizeof(CT);
-      if (ws.hadamard_smem < smem) {
-        XCUDA(cudaFuncSetAttribute(k_hadamard<CT, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        ws.hadamard_smem = smem;
+      const int ntiles = ws.had_tile0[g + 1] - ws.had_tile0[g];
+      if constexpr (sizeof(CT) == 8) {
+        const size_t smem = (size_t)26 * 64 * sizeof(float4) + (size_t)HADR_TT * HADR_RST * sizeof(float);
+        if (ws.hadamard_smem < smem) {
+          XCUDA(cudaFuncSetAttribute(k_hadamard_r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          ws.hadamard_smem = smem;
+        }
+        XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
+        k_hadamard_r<<<dim3(ntiles, nfreq), HADR_NT, smem, s>>>(T, (const CT*)ws.specB.p, (CT*)ws.specA.p,
+                                                               ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
+                                                               ws.hadr_ent.p, ns, nt, nfreq);
+      } else {
+        constexpr int KC = HadKC<CT>::KC;
+        using MT = typename HadM<CT>::type;
+        const size_t smem = (size_t)KC * 26 * 64 * sizeof(MT) + (size_t)KC * HAD_TT * HAD_ST * sizeof(CT);
+        if (ws.hadamard_smem < smem) {
+          XCUDA(cudaFuncSetAttribute(k_hadamard<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          ws.hadamard_smem = smem;
+        }
+        k_hadamard<CT><<<dim3(ntiles, (nfreq + KC - 1) / KC), 128 * KC, smem, s>>>(
+            T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.had_off.p + (int64_t)ws.had_tile0[g] * 4,
+            ws.had_pairs.p, ns, nt, nfreq);
       }
-      k_hadamard<CT, KC><<<(nfreq + KC - 1) / KC, 256, smem, s>>>(T, (const CT*)ws.specB.p, (CT*)ws.specA.p,
-                                                                    t.m2l_tab.p + (int64_t)t.m2l_trg_off[g] * 26, ns,
-                                                                    nt, nfreq);
       XLAUNCH();
       ws.launches++;
       XCUDA(cudaEventRecord(ev[2], s));
@@ -798,7 +1477,8 @@ struct Engine {
     for (int l = 0; l < t.depth; l++) {
       const GemmRows& g = ws.l2l[l];
       ws.launches++;
-        gemm_rows<W>(g.M, 8 * n, n, (const W*)ws.dn.p, g.a.p, ops_of<W>(f, l).l2l, (W*)ws.dn.p, g.c.p, nullptr, 1, s);
+        gemm_rows<W, W, W>(g.M, 8 * n, n, (const W*)ws.dn.p, g.a.p, ops_of<W, V64>(f, l).l2l, (W*)ws.dn.p, g.c.p,
+                           nullptr, 1, s);
     }
     XCUDA(cudaEventRecord(ws.ev[5], s));
     // L2P part 1: downward check -> equivalent (DC2E) per leaf level
@@ -809,23 +1489,35 @@ struct Engine {
         const int m = KER == K_LAPLACE ? ws.l2p1.M : r1 - r0;
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
-        const Ops<W> o = ops_of<W>(f, l);
+        const Ops<W, V64> o = ops_of<W, V64>(f, l);
         ws.launches++;
-        gemm_rows<W>(m, n, n, (const W*)ws.dn.p, ws.l2p1.a.p + off, o.l2p1, (W*)ws.chk.p, ws.l2p1.c.p + off,
-                     nullptr, 0, s);
+        gemm_rows<W, V64, V64>(m, n, n, (const W*)ws.dn.p, ws.l2p1.a.p + off, o.l2p1, (V64*)ws.ybuf.p,
+                               ws.l2p1.c.p + off, nullptr, 0, s);
         ws.launches++;
-        gemm_rows<W>(m, n, n, (const W*)ws.chk.p, ws.l2p2.a.p + off, o.l2p2, (W*)ws.eq.p, ws.l2p2.c.p + off,
-                     alpha_of<R>(ws.l2p2) + off, 0, s);
+        gemm_rows<V64, V64, V64>(m, n, n, (const V64*)ws.ybuf.p, ws.l2p2.a.p + off, o.l2p2, (V64*)ws.eq.p,
+                                 ws.l2p2.c.p + off, alpha_of<double>(ws.l2p2) + off, 0, s);
       }
     }
     XCUDA(cudaEventRecord(ws.ev[6], s));
-    // P2P + M2P + L2P target evaluation
+    // Target evaluation: the near field (P2P) in the working precision (FP32 with hi/lo coordinates when
+    // mixed), then the far field (M2P + L2P: sums of cancelling equivalent charges) in FP64, accumulated.
     if (t.n_eval_leafs) {
       EvalArgs a{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.level.p,     t.n_eval_leafs, t.sbeg.p,
                  t.tbeg.p,       t.center.p, t.src4.p,   t.trg4.p,  t.src_qim.p,   t.p2p_off.p,    t.m2p_off.p,
                  t.p2p.p,        t.m2p.p,   f.surf_base.p, n,        ws.up.p,       ws.eq.p,        ws.out.p,
                  f.k_re,         f.k_im,    1,           1,         0,             1};
-      k_eval<KER, R><<<nblk(t.n_eval_leafs, EVAL_WARPS), 32 * EVAL_WARPS, 0, s>>>(a);
+      const int blocks = nblk(t.n_eval_leafs, EVAL_WARPS);
+      NearArgs na{t.eval_leafs.p, t.leafs.p, t.nsrcs.p, t.ntrgs.p, t.n_eval_leafs, t.sbeg.p, t.tbeg.p, t.p2p_off.p,
+                  t.p2p.p,        t.center.p, t.src4.p, t.trg4.p, t.src_qim.p,    ws.out.p, f.k_re,   f.k_im};
+      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
+        k_near_lap_f2<<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
+      else
+        k_near<KER, R><<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
+      XLAUNCH();
+      ws.launches++;
+      a.do_near = 0;
+      a.accumulate = 1;
+      k_eval<KER, double, W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
       XLAUNCH();
       ws.launches++;
     }

@@ -349,10 +349,11 @@ void precompute(Fmm& f, int depth, cudaStream_t s) {
       }
     }
     // ---- GEMM operands in the working precision
+    // the check-to-equivalent factors stay FP64 in both precisions
     DBuf<char>* dst[4] = {&op.p2m_B1, &op.p2m_B2, &op.l2p_B1, &op.l2p_B2};
     for (int i = 0; i < 4; i++) {
-      dst[i]->alloc((size_t)n * n * wsz);
-      k_place<<<nb((int64_t)n * n), 256, 0, s>>>(F[i].p, n, 0, cplx, n, 0, 0, dst[i]->p, single);
+      dst[i]->alloc((size_t)n * n * vs * sizeof(double));
+      XCUDA(cudaMemcpyAsync(dst[i]->p, F[i].p, (size_t)n * n * vs * sizeof(double), cudaMemcpyDeviceToDevice, s));
     }
     op.m2m_B.alloc((size_t)8 * n * n * wsz);
     op.l2l_B.alloc((size_t)8 * n * n * wsz);

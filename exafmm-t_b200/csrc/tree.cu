@@ -902,6 +902,7 @@ void m2l_setup(Fmm& fmm, Tree& t, cudaStream_t s) {
   t.m2l_src.upload(src, s);
   t.m2l_trg.upload(trg, s);
   t.m2l_tab.upload(tab, s);
+  t.h_m2l_tab = tab;
   t.m2l_scale.upload(scale, s);
   t.m2l_scale64.upload(scale64, s);
   XCUDA(cudaStreamSynchronize(s));

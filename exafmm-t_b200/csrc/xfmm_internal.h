@@ -139,6 +139,7 @@ struct Tree {
   DBuf<int> m2l_trg;                  // targets (nonleaf node idx), same grouping
   std::vector<int> m2l_trg_off;
   DBuf<int> m2l_tab;                  // [n_trg][26] compact source index within its group, -1 if none
+  std::vector<int> h_m2l_tab;
   DBuf<float> m2l_scale;              // per target 2^(level+1) (Laplace) else 1
   DBuf<double> m2l_scale64;
   int n_m2l_src = 0, n_m2l_trg = 0;
@@ -149,7 +150,7 @@ struct Tree {
 // Precomputed operators of one level (or the single scale-invariant level).
 struct LevelOps {
   // working precision copies (float for mixed, double for fp64); complex types stored as interleaved pairs
-  // K(check, equiv) = U S V^H; the pseudo-inverse is applied in two factors exactly as the
+  // K(check, equiv) = U S V^H; the pseudo-inverse is applied in FP64 (both precisions), in two factors as the
   // reference does (UC2E_U then UC2E_V, DC2E_U then DC2E_V), never as one product: P = V S+ U^H
   // has entries up to ~1/s_min and a single dot product with it cancels catastrophically.
   DBuf<char> p2m_B1;   // [n][n]      y = U^H c        : B1[k][j] = conj(U[k][j])

@@ -7,7 +7,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(HERE), "libexafmm_b200.so")
+# XFMM_LIBRARY overrides the library file (e.g. a build with other compile-time tile sizes)
+LIB_PATH = os.environ.get("XFMM_LIBRARY") or os.path.join(os.path.dirname(HERE), "libexafmm_b200.so")
 
 STATUS = {
     0: "OK", 1: "invalid argument", 2: "out of memory", 3: "CUDA error", 4: "device wait timed out",
