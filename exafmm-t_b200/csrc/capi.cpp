@@ -60,6 +60,8 @@ void check_finite_host(const double* a, size_t n, const char* what) {
 }
 }  // namespace
 
+void xfmm::set_last_error(const char* msg) { g_err = msg; }
+
 extern "C" {
 
 const char* xfmm_last_error(void) { return g_err.c_str(); }

@@ -1703,6 +1703,32 @@ void gradient_p2p_raw(int kernel, double k_re, double k_im, int precision, const
   XCUDA(cudaStreamSynchronize(s));
 }
 
+// The evaluation of gradient_p2p_raw with the packed bodies in device scratch that the caller owns
+// (s4: ns double4, qim: ns doubles, t4: nt double4, each 32-byte aligned).  Asynchronous on s; no
+// allocation and no synchronisation.  The packing kernels write every scratch entry the P2P kernel
+// reads, so the scratch needs no initial contents.
+void gradient_p2p_scratch(int kernel, double k_re, double k_im, int precision, const double* src, int64_t ns,
+                          const double* q, const double* trg, int64_t nt, double* out, double4* s4, double* qim,
+                          double4* t4, cudaStream_t s) {
+  const int cplx = kernel == XFMM_HELMHOLTZ;
+  if (ns > 0) k_pack_raw<<<nblk(ns), 256, 0, s>>>(src, q, ns, cplx, s4, qim);
+  k_pack_raw<<<nblk(nt), 256, 0, s>>>(trg, nullptr, nt, 0, t4, nullptr);
+  XLAUNCH();
+  const int blocks = nblk(nt, 128);
+  const bool m = precision == XFMM_MIXED;
+  if (kernel == XFMM_LAPLACE) {
+    if (m) k_raw_p2p<K_LAPLACE, float><<<blocks, 128, 0, s>>>(s4, qim, ns, t4, nt, k_re, k_im, out);
+    else k_raw_p2p<K_LAPLACE, double><<<blocks, 128, 0, s>>>(s4, qim, ns, t4, nt, k_re, k_im, out);
+  } else if (kernel == XFMM_MODIFIED_HELMHOLTZ) {
+    if (m) k_raw_p2p<K_YUKAWA, float><<<blocks, 128, 0, s>>>(s4, qim, ns, t4, nt, k_re, k_im, out);
+    else k_raw_p2p<K_YUKAWA, double><<<blocks, 128, 0, s>>>(s4, qim, ns, t4, nt, k_re, k_im, out);
+  } else {
+    if (m) k_raw_p2p<K_HELMHOLTZ, float><<<blocks, 128, 0, s>>>(s4, qim, ns, t4, nt, k_re, k_im, out);
+    else k_raw_p2p<K_HELMHOLTZ, double><<<blocks, 128, 0, s>>>(s4, qim, ns, t4, nt, k_re, k_im, out);
+  }
+  XLAUNCH();
+}
+
 // FmmBase::verify (fmm_base.h:208-267) on the device: FP64 direct sum over all sources
 void verify(Fmm& f, Tree& t, int sample, double* err2, cudaStream_t s) {
   Workspace& ws = workspace(f, t, s);

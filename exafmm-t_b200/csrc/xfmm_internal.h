@@ -199,5 +199,10 @@ void stage_times(Fmm& fmm, Tree& t, double* ms12);
 void gradient_p2p_raw(int kernel, double k_re, double k_im, int precision, const double* src, int64_t ns,
                       const double* q, const double* trg, int64_t nt, double* out, cudaStream_t s);
 void verify(Fmm& fmm, Tree& t, int sample, double* err2, cudaStream_t s);
+void gradient_p2p_scratch(int kernel, double k_re, double k_im, int precision, const double* src, int64_t ns,
+                          const double* q, const double* trg, int64_t nt, double* out, double4* s4, double* qim,
+                          double4* t4, cudaStream_t s);
+// capi.cpp: record the message returned by xfmm_last_error() on this thread
+void set_last_error(const char* msg);
 
 }  // namespace xfmm

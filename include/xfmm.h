@@ -117,6 +117,22 @@ xfmm_status xfmm_gradient_p2p(int kernel, double k_re, double k_im, int precisio
                               int64_t nsrc, const double* q, const double* trg_xyz, int64_t ntrg, double* out,
                               int on_device, void* stream);
 
+/* Size of the fixed device scratch of xfmm_gradient_p2p_noalloc (16 MiB): 40 bytes per source and
+ * 32 per target, each region rounded up to 256 bytes. */
+#define XFMM_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* xfmm_gradient_p2p with device pointers only and no allocation: the packed bodies live in one
+ * static device array per device instead of memory allocated per call.  No counterpart in the
+ * reference (its gradient_P2P, include/laplace.h:91-164, is a host loop).  For callers that must not
+ * allocate device memory while they run (allocation can synchronise the device; their memory pool
+ * is fixed at start-up).  The first call on each device looks the array up (make it before any
+ * stream capture begins); sizes beyond XFMM_NOALLOC_SCRATCH_BYTES return XFMM_ERR_ARG; out is
+ * accumulated into (start it at zero for the plain result); the scratch needs no initial contents;
+ * the call is asynchronous on stream; overlapping calls on one device share the scratch and race. */
+xfmm_status xfmm_gradient_p2p_noalloc(int kernel, double k_re, double k_im, int precision, const double* src_xyz,
+                                      int64_t nsrc, const double* q, const double* trg_xyz, int64_t ntrg,
+                                      double* out, void* stream);
+
 /* FmmBase::verify on the device: relative L2 error of potential and gradient of the last
  * evaluate against FP64 direct summation over all sources, on every target (sample == 0)
  * or the targets of 10 leaves at stride nleafs/10 (sample != 0). */
