@@ -902,132 +902,195 @@ __global__ void __launch_bounds__(128 * HadKC<CT>::KC) k_hadamard(const CT* __re
 // Hadamard product, round form (FP32 working precision).  The same product as k_hadamard, scheduled
 // for targets with few interactions: a CTA owns HADR_TT targets at one frequency; the tile's pairs are
 // grouped by relative position and packed on the host into rounds of HADR_RW pairs that share one
-// position, so a warp reads the 8x8 block of that position once (a shared-memory broadcast) for the
-// two pairs each lane holds.  Any warp may take any round; targets repeat across concurrent rounds of
-// different positions, so the accumulators are updated with shared-memory atomics (the FP32 sums are
-// therefore taken in a run-dependent order).  Two FP32 operations per instruction (__ffma2_rn), with
-// the 8x8 blocks expanded in shared memory to {re, re, -im, im}.
-#ifndef XFMM_HADR_PREFETCH
-#define XFMM_HADR_PREFETCH 1
+// position, so a warp reads each entry of that position's 8x8 block once (a shared-memory broadcast)
+// for the HADR_PPL pairs each lane holds.  Any warp may take any round; targets repeat across
+// concurrent rounds of different positions, so the accumulators are updated with shared-memory
+// atomics (the FP32 sums are therefore taken in a run-dependent order).  Two FP32 operations per
+// instruction (__ffma2_rn), with the 8x8 blocks expanded in shared memory to {re, re, -im, im}; the
+// 8 outputs of a pair are computed in HADR_NH passes to bound the registers held per lane.
+#ifndef XFMM_HADR_TT
+#define XFMM_HADR_TT 512
 #endif
-constexpr int HADR_NT = 256;            // threads per CTA
-constexpr int HADR_TT = 1024;           // targets per tile
-constexpr int HADR_RST = 17;            // accumulator stride per target in reals (16 values + 1 pad)
-constexpr int HADR_PPL = 2;             // pairs per lane per round
-constexpr int HADR_RW = 32 * HADR_PPL;  // pairs per round
+#ifndef XFMM_HADR_MINB
+#define XFMM_HADR_MINB 3
+#endif
+#ifndef XFMM_HADR_PPL
+#define XFMM_HADR_PPL 2
+#endif
+#ifndef XFMM_HADR_NH
+#define XFMM_HADR_NH 2
+#endif
+constexpr int HADR_NT = 256;                 // threads per CTA
+constexpr int HADR_TT = XFMM_HADR_TT;        // targets per tile
+constexpr int HADR_AS = HADR_TT + 1;         // accumulator row stride: [16 components][HADR_TT + 1]
+constexpr int HADR_PPL = XFMM_HADR_PPL;      // pairs per lane per round
+constexpr int HADR_RW = 32 * HADR_PPL;       // pairs per round
+constexpr int HADR_NH = XFMM_HADR_NH;        // output passes per round
+constexpr size_t hadr_smem() { return (size_t)26 * 64 * sizeof(float4) + (size_t)16 * HADR_AS * sizeof(float); }
+
+__global__ void __launch_bounds__(HADR_NT, XFMM_HADR_MINB)
+    k_hadamard_r(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
+                 const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
+                 const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
+  constexpr int NW = HADR_NT / 32, TC = 8 / HADR_NH;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sM = reinterpret_cast<float4*>(smem_raw);       // [26][64]
+  float* sAcc = reinterpret_cast<float*>(sM + 26 * 64);  // [16][HADR_AS]
+  const int tile = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
+  const int lane = tid & 31, wid = tid >> 5;
+  const int t0 = tile * HADR_TT;
+  for (int e = tid; e < 26 * 64; e += HADR_NT) {
+    const int j = e & 63, ipos = e >> 6;
+    const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + j];
+    sM[e] = make_float4(m.x, m.x, -m.y, m.y);
+  }
+  for (int e = tid; e < 16 * HADR_AS; e += HADR_NT) sAcc[e] = 0.f;
+  __syncthreads();
+  const float2* inf = in + (int64_t)f * nsrc * 8;
+  const int r1 = tile_r[tile + 1];
+  for (int r = tile_r[tile] + wid; r < r1; r += NW) {
+    const float4* M = sM + rpos[r] * 64;
+    int2 c[HADR_PPL];
+    float2 v[HADR_PPL][8];
+#pragma unroll
+    for (int p = 0; p < HADR_PPL; p++) {
+      c[p] = ent[(int64_t)r * HADR_RW + 32 * p + lane];
+      if (c[p].x >= 0) {
+        had_load8<float2>(inf + (int64_t)c[p].x * 8, v[p]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[p][i] = make_float2(0.f, 0.f);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < HADR_NH; h++) {
+      float2 o[HADR_PPL][TC];
+#pragma unroll
+      for (int p = 0; p < HADR_PPL; p++)
+#pragma unroll
+        for (int i = 0; i < TC; i++) o[p][i] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int sc = 0; sc < 8; sc++) {
+#pragma unroll
+        for (int i = 0; i < TC; i++) {
+          const float4 m = M[sc * 8 + h * TC + i];  // {re, re, -im, im}
+          const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
+#pragma unroll
+          for (int p = 0; p < HADR_PPL; p++) {
+            o[p][i] = __ffma2_rn(mr, v[p][sc], o[p][i]);
+            o[p][i] = __ffma2_rn(mi, make_float2(v[p][sc].y, v[p][sc].x), o[p][i]);
+          }
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < HADR_PPL; p++) {
+        if (c[p].x < 0) continue;
+        float* q = sAcc + c[p].y;
+#pragma unroll
+        for (int i = 0; i < TC; i++) {
+          atomicAdd(q + (2 * (h * TC + i)) * HADR_AS, o[p][i].x);
+          atomicAdd(q + (2 * (h * TC + i) + 1) * HADR_AS, o[p][i].y);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  float2* of = out + (int64_t)f * ntrg * 8;
+  for (int e = tid; e < HADR_TT * 8; e += HADR_NT) {
+    const int t = e >> 3, comp = 2 * (e & 7), row = rows[t0 + t];
+    if (row >= 0) of[(int64_t)row * 8 + (e & 7)] = make_float2(sAcc[comp * HADR_AS + t], sAcc[(comp + 1) * HADR_AS + t]);
+  }
+}
+
+// Hadamard product, dense form (FP32 working precision), for targets with most of the 26 relative
+// positions occupied.  A warp owns 64 targets (two per lane) and walks the 26 positions in order:
+// each lane multiplies its two targets' source spectra (zeros where a position is empty) by that
+// position's 8x8 block, read once per warp as a shared-memory broadcast, and keeps the sums in
+// registers, so there are no shared accumulators and no atomics; the sums are taken in a fixed order.
+// The next position's spectra are loaded while the current one is multiplied.
+#ifndef XFMM_HAD_DENSE_MIN
+#define XFMM_HAD_DENSE_MIN 12
+#endif
+constexpr int HADD_NT = 256;                 // threads per CTA
+constexpr int HADD_TT = 2 * HADD_NT;         // targets per CTA
+constexpr int HAD_DENSE_MIN = XFMM_HAD_DENSE_MIN;  // occupied positions that make a target dense
 
 __device__ __forceinline__ void had_mac8x2(const float4* __restrict__ M, const float2* v0, const float2* v1,
                                            float2* o0, float2* o1) {
 #pragma unroll
   for (int sc = 0; sc < 8; sc++) {
-    const float2 a0 = v0[sc], b0 = make_float2(v0[sc].y, v0[sc].x);
-    const float2 a1 = v1[sc], b1 = make_float2(v1[sc].y, v1[sc].x);
+    const float2 b0 = make_float2(v0[sc].y, v0[sc].x), b1 = make_float2(v1[sc].y, v1[sc].x);
 #pragma unroll
     for (int tc = 0; tc < 8; tc++) {
       const float4 m = M[sc * 8 + tc];  // {re, re, -im, im}
       const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
-      o0[tc] = __ffma2_rn(mr, a0, o0[tc]);
-      o1[tc] = __ffma2_rn(mr, a1, o1[tc]);
+      o0[tc] = __ffma2_rn(mr, v0[sc], o0[tc]);
+      o1[tc] = __ffma2_rn(mr, v1[sc], o1[tc]);
       o0[tc] = __ffma2_rn(mi, b0, o0[tc]);
       o1[tc] = __ffma2_rn(mi, b1, o1[tc]);
     }
   }
 }
 
-__global__ void __launch_bounds__(HADR_NT, 2) k_hadamard_r(const float2* __restrict__ T, const float2* __restrict__ in,
-                                                           float2* __restrict__ out, const int* __restrict__ tile_r,
-                                                           const int* __restrict__ rpos, const int2* __restrict__ ent,
-                                                           int nsrc, int ntrg, int nfreq) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* sM = reinterpret_cast<float4*>(smem_raw);           // [26][64]
-  float* sAcc = reinterpret_cast<float*>(sM + 26 * 64);      // [HADR_TT][HADR_RST]
-  constexpr int NW = HADR_NT / 32;
-  const int tile = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
-  const int lane = tid & 31, wid = tid >> 5;
-  const int t0 = tile * HADR_TT, nt = min(HADR_TT, ntrg - t0);
-  for (int e = tid; e < 26 * 64; e += HADR_NT) {
+__device__ __forceinline__ void had_load8_or_zero(const float2* __restrict__ inf, int src, float2* v) {
+  if (src >= 0) {
+    had_load8<float2>(inf + (int64_t)src * 8, v);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = make_float2(0.f, 0.f);
+  }
+}
+
+// tab: [26][ld] compact source index of dense target k at each position (-1: empty or padding);
+// rows: [ld] output row of dense target k (-1: padding).  ld is a multiple of HADD_TT.
+__global__ void __launch_bounds__(HADD_NT, 2)
+    k_hadamard_d(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
+                 const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
+  __shared__ float4 sM[26 * 64];
+  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int e = tid; e < 26 * 64; e += HADD_NT) {
     const int j = e & 63, ipos = e >> 6;
     const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + j];
     sM[e] = make_float4(m.x, m.x, -m.y, m.y);
   }
-  for (int e = tid; e < nt * HADR_RST; e += HADR_NT) sAcc[e] = 0.f;
   __syncthreads();
+  const int ka = blockIdx.x * HADD_TT + wid * 64 + lane, kb = ka + 32;
   const float2* inf = in + (int64_t)f * nsrc * 8;
-  const int r1 = tile_r[tile + 1];
-  int r = tile_r[tile] + wid;
-  int2 c0 = make_int2(-1, 0), c1 = make_int2(-1, 0);
-  int cpos = 0;
-  float2 v0[8], v1[8];
+  float2 oa[8], ob[8], va[8], vb[8];
 #pragma unroll
-  for (int i = 0; i < 8; i++) v0[i] = v1[i] = make_float2(0.f, 0.f);
-  if (r < r1) {
-    cpos = rpos[r];
-    c0 = ent[(int64_t)r * HADR_RW + lane];
-    c1 = ent[(int64_t)r * HADR_RW + 32 + lane];
-#if XFMM_HADR_PREFETCH
-    if (c0.x >= 0) had_load8<float2>(inf + (int64_t)c0.x * 8, v0);
-    if (c1.x >= 0) had_load8<float2>(inf + (int64_t)c1.x * 8, v1);
-#endif
-  }
-  for (; r < r1; r += NW) {
-    // prefetch this warp's next round (its pairs, and with XFMM_HADR_PREFETCH their inputs) while
-    // computing the current one
-    const int rn = r + NW;
-    int2 n0 = make_int2(-1, 0), n1 = make_int2(-1, 0);
-    int npos = 0;
-#if XFMM_HADR_PREFETCH
-    float2 w0[8], w1[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) w0[i] = w1[i] = make_float2(0.f, 0.f);
-#else
-    if (c0.x >= 0) had_load8<float2>(inf + (int64_t)c0.x * 8, v0);
-    if (c1.x >= 0) had_load8<float2>(inf + (int64_t)c1.x * 8, v1);
-#endif
-    if (rn < r1) {
-      npos = rpos[rn];
-      n0 = ent[(int64_t)rn * HADR_RW + lane];
-      n1 = ent[(int64_t)rn * HADR_RW + 32 + lane];
-#if XFMM_HADR_PREFETCH
-      if (n0.x >= 0) had_load8<float2>(inf + (int64_t)n0.x * 8, w0);
-      if (n1.x >= 0) had_load8<float2>(inf + (int64_t)n1.x * 8, w1);
-#endif
+  for (int i = 0; i < 8; i++) oa[i] = ob[i] = make_float2(0.f, 0.f);
+  int sa = tab[ka], sb = tab[kb];
+  had_load8_or_zero(inf, sa, va);
+  had_load8_or_zero(inf, sb, vb);
+  for (int ipos = 0; ipos < 26; ipos++) {
+    int na = -1, nb = -1;
+    if (ipos + 1 < 26) {
+      na = tab[(ipos + 1) * ld + ka];
+      nb = tab[(ipos + 1) * ld + kb];
     }
-    float2 o0[8], o1[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) o0[i] = o1[i] = make_float2(0.f, 0.f);
-    had_mac8x2(sM + cpos * 64, v0, v1, o0, o1);
-    if (c0.x >= 0) {
-      float* q = sAcc + c0.y * HADR_RST;
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        atomicAdd(q + 2 * i, o0[i].x);
-        atomicAdd(q + 2 * i + 1, o0[i].y);
-      }
-    }
-    if (c1.x >= 0) {
-      float* q = sAcc + c1.y * HADR_RST;
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        atomicAdd(q + 2 * i, o1[i].x);
-        atomicAdd(q + 2 * i + 1, o1[i].y);
-      }
-    }
-    c0 = n0;
-    c1 = n1;
-    cpos = npos;
-#if XFMM_HADR_PREFETCH
+    float2 wa[8], wb[8];
+    had_load8_or_zero(inf, na, wa);
+    had_load8_or_zero(inf, nb, wb);
+    if (__any_sync(0xffffffffu, (sa >= 0) | (sb >= 0))) had_mac8x2(sM + ipos * 64, va, vb, oa, ob);
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-      v0[i] = w0[i];
-      v1[i] = w1[i];
+      va[i] = wa[i];
+      vb[i] = wb[i];
     }
-#endif
+    sa = na;
+    sb = nb;
   }
-  __syncthreads();
-  float2* of = out + ((int64_t)f * ntrg + t0) * 8;
-  for (int e = tid; e < nt * 8; e += HADR_NT) {
-    const float* a = sAcc + (e >> 3) * HADR_RST + 2 * (e & 7);
-    of[e] = make_float2(a[0], a[1]);
+  float2* of = out + (int64_t)f * ntrg * 8;
+  const int ra = rows[ka], rb = rows[kb];
+  if (ra >= 0) {
+    float4* q = reinterpret_cast<float4*>(of + (int64_t)ra * 8);
+#pragma unroll
+    for (int i = 0; i < 4; i++) q[i] = make_float4(oa[2 * i].x, oa[2 * i].y, oa[2 * i + 1].x, oa[2 * i + 1].y);
+  }
+  if (rb >= 0) {
+    float4* q = reinterpret_cast<float4*>(of + (int64_t)rb * 8);
+#pragma unroll
+    for (int i = 0; i < 4; i++) q[i] = make_float4(ob[2 * i].x, ob[2 * i].y, ob[2 * i + 1].x, ob[2 * i + 1].y);
   }
 }
 
@@ -1094,9 +1157,14 @@ struct Workspace {
   DBuf<int> had_off;
   DBuf<int2> had_pairs;
   std::vector<int> had_tile0;  // first tile of each group (ngroups + 1)
-  // round form (FP32): per tile the range of rounds; per round its relative position and HADR_RW pairs
-  DBuf<int> hadr_tile, hadr_pos;
+  // FP32: sparse targets in the round form (per tile the range of rounds and HADR_TT output rows; per
+  // round its relative position and HADR_RW pairs), dense targets in the dense form (per group a
+  // [26][ld] source table and ld output rows)
+  DBuf<int> hadr_tile, hadr_pos, hadr_row;
   DBuf<int2> hadr_ent;
+  DBuf<int> hadd_tab, hadd_row;
+  std::vector<int64_t> hadd_tab0, hadd_row0;
+  std::vector<int> hadd_ld;
   size_t hadamard_smem = 0;
   int64_t launches = 0;  // kernels of this library launched by the last evaluate
   cudaEvent_t ev[8] = {};
@@ -1227,29 +1295,53 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
     W.bwd.push_back(hb);
   }
   if (f.mixed()) {
-    // round form: per group, tiles of HADR_TT targets; per tile and relative position the pairs
-    // (source index, target index within the tile) in rounds of HADR_RW, padded with source -1.
-    std::vector<int> tile_r, pos;
+    // Targets with at least HAD_DENSE_MIN occupied positions go to the dense form, in tiles of HADD_TT
+    // (table [26][ld], padded with -1).  The others go to the round form: tiles of HADR_TT targets;
+    // per tile and relative position the pairs (source index, target index within the tile) in rounds
+    // of HADR_RW, padded with source -1.  Both write disjoint rows of the group's output.
+    std::vector<int> tile_r, pos, srow, dtab, drow;
     std::vector<int2> ent;
     W.had_tile0.assign(ng + 1, 0);
+    W.hadd_tab0.assign(ng, 0);
+    W.hadd_row0.assign(ng, 0);
+    W.hadd_ld.assign(ng, 0);
     int ntiles = 0;
     for (int g = 0; g < ng; g++) {
       W.had_tile0[g] = ntiles;
       const int tb = t.m2l_trg_off[g], te = t.m2l_trg_off[g + 1];
-      for (int t0 = tb; t0 < te; t0 += HADR_TT, ntiles++) {
+      std::vector<int> dense, sparse;
+      for (int tt = tb; tt < te; tt++) {
+        int cnt = 0;
+        for (int ipos = 0; ipos < 26; ipos++) cnt += t.h_m2l_tab[26 * (size_t)tt + ipos] >= 0;
+        (cnt >= HAD_DENSE_MIN ? dense : sparse).push_back(tt);
+      }
+      const int ld = (int)((dense.size() + HADD_TT - 1) / HADD_TT) * HADD_TT;
+      W.hadd_ld[g] = ld;
+      W.hadd_tab0[g] = (int64_t)dtab.size();
+      W.hadd_row0[g] = (int64_t)drow.size();
+      dtab.resize(dtab.size() + (size_t)26 * ld, -1);
+      drow.resize(drow.size() + ld, -1);
+      for (size_t k = 0; k < dense.size(); k++) {
+        const int tt = dense[k];
+        drow[W.hadd_row0[g] + k] = tt - tb;
+        for (int ipos = 0; ipos < 26; ipos++)
+          dtab[W.hadd_tab0[g] + (size_t)ipos * ld + k] = t.h_m2l_tab[26 * (size_t)tt + ipos];
+      }
+      for (size_t k0 = 0; k0 < sparse.size(); k0 += HADR_TT, ntiles++) {
         tile_r.push_back((int)pos.size());
-        const int t1 = std::min(te, t0 + HADR_TT);
+        const size_t k1 = std::min(sparse.size(), k0 + HADR_TT);
+        for (size_t k = k0; k < k0 + HADR_TT; k++) srow.push_back(k < k1 ? sparse[k] - tb : -1);
         for (int ipos = 0; ipos < 26; ipos++) {
-          int k = 0;
-          for (int tt = t0; tt < t1; tt++) {
-            const int sidx = t.h_m2l_tab[26 * (size_t)tt + ipos];
+          int n = 0;
+          for (size_t k = k0; k < k1; k++) {
+            const int sidx = t.h_m2l_tab[26 * (size_t)sparse[k] + ipos];
             if (sidx < 0) continue;
-            if (k == 0) {
+            if (n == 0) {
               pos.push_back(ipos);
               ent.resize(ent.size() + HADR_RW, make_int2(-1, 0));
             }
-            ent[ent.size() - HADR_RW + k] = make_int2(sidx, tt - t0);
-            if (++k == HADR_RW) k = 0;
+            ent[ent.size() - HADR_RW + n] = make_int2(sidx, (int)(k - k0));
+            if (++n == HADR_RW) n = 0;
           }
         }
       }
@@ -1260,9 +1352,15 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
       pos.push_back(0);
       ent.resize(HADR_RW, make_int2(-1, 0));
     }
+    if (srow.empty()) srow.push_back(-1);
+    if (dtab.empty()) dtab.push_back(-1);
+    if (drow.empty()) drow.push_back(-1);
     W.hadr_tile.upload(tile_r, s);
     W.hadr_pos.upload(pos, s);
     W.hadr_ent.upload(ent, s);
+    W.hadr_row.upload(srow, s);
+    W.hadd_tab.upload(dtab, s);
+    W.hadd_row.upload(drow, s);
   } else {
     // per group of M2L targets: tiles of HAD_TT targets, 4 warp groups of 32 targets; each warp group's
     // pairs (ordered by relative position) packed into rounds of 32 lanes with no repeated target,
@@ -1402,15 +1500,26 @@ struct Engine {
       // Hadamard product
       const int ntiles = ws.had_tile0[g + 1] - ws.had_tile0[g];
       if constexpr (sizeof(CT) == 8) {
-        const size_t smem = (size_t)26 * 64 * sizeof(float4) + (size_t)HADR_TT * HADR_RST * sizeof(float);
+        const size_t smem = hadr_smem();
         if (ws.hadamard_smem < smem) {
           XCUDA(cudaFuncSetAttribute(k_hadamard_r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
           ws.hadamard_smem = smem;
         }
         XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
-        k_hadamard_r<<<dim3(ntiles, nfreq), HADR_NT, smem, s>>>(T, (const CT*)ws.specB.p, (CT*)ws.specA.p,
-                                                               ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
-                                                               ws.hadr_ent.p, ns, nt, nfreq);
+        if (ntiles > 0) {
+          k_hadamard_r<<<dim3(ntiles, nfreq), HADR_NT, smem, s>>>(
+              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
+              ws.hadr_ent.p, ws.hadr_row.p + (int64_t)ws.had_tile0[g] * HADR_TT, ns, nt, nfreq);
+          XLAUNCH();
+          ws.launches++;
+        }
+        if (ws.hadd_ld[g] > 0) {
+          k_hadamard_d<<<dim3(ws.hadd_ld[g] / HADD_TT, nfreq), HADD_NT, 0, s>>>(
+              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+              ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
+          XLAUNCH();
+          ws.launches++;
+        }
       } else {
         constexpr int KC = HadKC<CT>::KC;
         using MT = typename HadM<CT>::type;
@@ -1422,9 +1531,9 @@ struct Engine {
         k_hadamard<CT><<<dim3(ntiles, (nfreq + KC - 1) / KC), 128 * KC, smem, s>>>(
             T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.had_off.p + (int64_t)ws.had_tile0[g] * 4,
             ws.had_pairs.p, ns, nt, nfreq);
+        XLAUNCH();
+        ws.launches++;
       }
-      XLAUNCH();
-      ws.launches++;
       XCUDA(cudaEventRecord(ev[2], s));
       // inverse FFT to downward check potentials (fmm_scale_invariant.h:606-646)
       ws.launches++;
