@@ -1,17 +1,20 @@
 // evaluate.cu -- upward and downward passes of the KIFMM on the GPU.
 //
 // Stage map (reference -> here):
-//   P2M   fmm_scale_invariant.h:163-195 / fmm.h:156-185  k_p2m (check potentials) + gemm_rows (pinv, 0.5^l)
-//   M2M   fmm_scale_invariant.h:233-253 / fmm.h:221-241  gemm_rows per level, K = 8 nsurf (children contiguous)
+//   P2M   fmm_scale_invariant.h:163-195 / fmm.h:156-185  k_surf_pot (check potentials) + row gather, two FP64
+//                                                        library GEMMs (pinv factors), scaled scatter (0.5^l)
+//   M2M   fmm_scale_invariant.h:233-253 / fmm.h:221-241  row gather + library GEMM per level, K = 8 nsurf
 //   P2L   fmm_base.h:127-154                             k_p2l
 //   M2L   fmm_scale_invariant.h:407-440, 560-646;        k_m2l_grid_up + cuFFT + k_transpose + k_hadamard
 //         fmm.h:395-446, 631-788                         + k_transpose + cuFFT + k_m2l_gather_dn
-//   L2L   fmm_scale_invariant.h:256-275 / fmm.h:244-263  gemm_rows per level, N = 8 nsurf
-//   L2P   fmm_scale_invariant.h:198-230 / fmm.h:188-218  gemm_rows (pinv^T, 0.5^l) + k_eval (far part)
+//   L2L   fmm_scale_invariant.h:256-275 / fmm.h:244-263  row gather + library GEMM per level, N = 8 nsurf
+//   L2P   fmm_scale_invariant.h:198-230 / fmm.h:188-218  scaled row gather, two FP64 library GEMMs, scatter
+//                                                        + k_eval (far part)
 //   M2P   fmm_base.h:97-124                              k_eval (far part)
 //   P2P   fmm_base.h:82-94                               k_eval (near part)
 // The near and far target evaluations share one warp-per-leaf kernel; results stay in
 // tree order until get_values scatters them (python/exafmm.cpp:194-207).
+#include <cublas_v2.h>
 #include <cufft.h>
 
 #include <algorithm>
@@ -679,83 +682,60 @@ __global__ void __launch_bounds__(128) k_surf_pot(SurfPotArgs a) {
 }
 
 // ================================================================ translation GEMMs
-// C[coff[i] + j] (+)= alpha[i] * sum_k A[aoff[i] + k] * B[k*N + j]   (rows gathered/scattered)
-// computed in B's precision; A is converted on load and C on store.
-template <class TA, class TB, class TC, int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_gemm_rows(int M, int N, int K, const TA* __restrict__ A,
-                                                                      const int64_t* __restrict__ aoff,
-                                                                      const TB* __restrict__ B, TC* __restrict__ C,
-                                                                      const int64_t* __restrict__ coff,
-                                                                      const typename Base<TB>::type* __restrict__ alpha,
-                                                                      int accumulate) {
-  using RB = typename Base<TB>::type;
-  constexpr int NT = (BM / TM) * (BN / TN);
-  __shared__ TB As[BK][BM];
-  __shared__ TB Bs[BK][BN];
-  const int tid = threadIdx.x;
-  const int tx = tid % (BN / TN), ty = tid / (BN / TN);
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  TB acc[TM][TN];
-#pragma unroll
-  for (int i = 0; i < TM; i++)
-#pragma unroll
-    for (int j = 0; j < TN; j++) acc[i][j] = vzero<TB>();
-  for (int k0 = 0; k0 < K; k0 += BK) {
-    for (int e = tid; e < BM * BK; e += NT) {
-      const int r = e / BK, kk = e % BK;
-      const int row = m0 + r, k = k0 + kk;
-      As[kk][r] = (row < M && k < K) ? cvt<TB>(A[aoff[row] + k]) : vzero<TB>();
-    }
-    for (int e = tid; e < BK * BN; e += NT) {
-      const int kk = e / BN, cc = e % BN;
-      const int k = k0 + kk, col = n0 + cc;
-      Bs[kk][cc] = (k < K && col < N) ? B[(int64_t)k * N + col] : vzero<TB>();
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < BK; kk++) {
-      TB av[TM], bv[TN];
-#pragma unroll
-      for (int i = 0; i < TM; i++) av[i] = As[kk][ty * TM + i];
-#pragma unroll
-      for (int j = 0; j < TN; j++) bv[j] = Bs[kk][tx * TN + j];
-#pragma unroll
-      for (int i = 0; i < TM; i++)
-#pragma unroll
-        for (int j = 0; j < TN; j++) vfma(acc[i][j], av[i], bv[j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < TM; i++) {
-    const int row = m0 + ty * TM + i;
-    if (row >= M) continue;
-    const RB al = alpha ? alpha[row] : RB(1);
-    TC* crow = C + coff[row];
-#pragma unroll
-    for (int j = 0; j < TN; j++) {
-      const int col = n0 + tx * TN + j;
-      if (col < N) {
-        const TB v = vscale(acc[i][j], al);
-        crow[col] = accumulate ? cvt<TC>(vadd(cvt<TB>(crow[col]), v)) : cvt<TC>(v);
-      }
-    }
+// Row gather / scatter around the library GEMMs: the rows of an operator application live at scattered
+// offsets (leaf and node rows of up/dn/chk/eq), the GEMMs want them contiguous.
+//   gather:  dst[r][j]           = alpha_r * src[aoff[r] + j]   (scaled in the destination type)
+//   scatter: dst[coff[r] + j] (+)= alpha_r * src[r][j]          (scaled in the source type)
+template <class TS, class TD>
+__global__ void k_rows_gather(int m, int n, const TS* __restrict__ src, const int64_t* __restrict__ aoff,
+                              const double* __restrict__ alpha, TD* __restrict__ dst) {
+  const int64_t total = (int64_t)m * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / n), j = (int)(e - (int64_t)r * n);
+    TD v = cvt<TD>(src[aoff[r] + j]);
+    if (alpha) v = vscale(v, (typename Base<TD>::type)alpha[r]);
+    dst[e] = v;
   }
 }
-
-template <class TA, class TB, class TC>
-void gemm_rows(int M, int N, int K, const TA* A, const int64_t* aoff, const TB* B, TC* C, const int64_t* coff,
-               const typename Base<TB>::type* alpha, int accumulate, cudaStream_t s) {
-  if (M <= 0) return;
-  constexpr bool cplx = sizeof(TB) == 2 * sizeof(typename Base<TB>::type);
-  if constexpr (cplx) {
-    dim3 grid((N + 63) / 64, (M + 31) / 32);
-    k_gemm_rows<TA, TB, TC, 32, 64, 8, 2, 4><<<grid, 256, 0, s>>>(M, N, K, A, aoff, B, C, coff, alpha, accumulate);
-  } else {
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
-    k_gemm_rows<TA, TB, TC, 64, 64, 16, 4, 4><<<grid, 256, 0, s>>>(M, N, K, A, aoff, B, C, coff, alpha, accumulate);
+template <class TS, class TD>
+__global__ void k_rows_scatter(int m, int n, const TS* __restrict__ src, const int64_t* __restrict__ coff,
+                               const double* __restrict__ alpha, TD* __restrict__ dst, int accumulate) {
+  const int64_t total = (int64_t)m * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / n), j = (int)(e - (int64_t)r * n);
+    TS v = src[e];
+    if (alpha) v = vscale(v, (typename Base<TS>::type)alpha[r]);
+    TD* d = dst + coff[r] + j;
+    *d = accumulate ? vadd(*d, cvt<TD>(v)) : cvt<TD>(v);
   }
-  XLAUNCH();
+}
+inline int rows_grid(int64_t total) { return (int)std::min<int64_t>(nblk(total), 148 * 16); }
+
+#define XCUBLAS2(call)                                                                               \
+  do {                                                                                               \
+    cublasStatus_t st_ = (call);                                                                     \
+    if (st_ != CUBLAS_STATUS_SUCCESS)                                                                \
+      throw Error(XFMM_ERR_CUDA, std::string("cuBLAS ") + #call + " failed: " + std::to_string((int)st_)); \
+  } while (0)
+
+// Row-major C[m][n] = A[m][k] B[k][n] with the library GEMM (column-major: C^T = B^T A^T).
+inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const float* A, const float* B, float* C) {
+  const float one = 1.f, zero = 0.f;
+  XCUBLAS2(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, B, n, A, k, &zero, C, n));
+}
+inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const double* A, const double* B, double* C) {
+  const double one = 1.0, zero = 0.0;
+  XCUBLAS2(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, B, n, A, k, &zero, C, n));
+}
+inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const float2* A, const float2* B, float2* C) {
+  const cuComplex one = make_cuComplex(1.f, 0.f), zero = make_cuComplex(0.f, 0.f);
+  XCUBLAS2(cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, (const cuComplex*)B, n, (const cuComplex*)A, k,
+                       &zero, (cuComplex*)C, n));
+}
+inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const double2* A, const double2* B, double2* C) {
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  XCUBLAS2(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, (const cuDoubleComplex*)B, n,
+                       (const cuDoubleComplex*)A, k, &zero, (cuDoubleComplex*)C, n));
 }
 
 // ================================================================ M2L
@@ -1136,7 +1116,6 @@ __global__ void k_scatter_out(const double* __restrict__ in, const int* __restri
 struct GemmRows {
   int M = 0;
   DBuf<int64_t> a, c;
-  DBuf<float> al32;
   DBuf<double> al64;
 };
 
@@ -1145,6 +1124,9 @@ struct Workspace {
   size_t vsz = 0;
   DBuf<char> up, dn, chk;  // working precision
   DBuf<char> ybuf, eq;     // FP64: pinv intermediate, downward equivalent densities of the leaves
+  DBuf<char> xbuf;         // FP64: pinv input rows / output rows (contiguous, in leaf-level order)
+  DBuf<char> wA, wC;       // working precision: M2M/L2L input and output rows (contiguous)
+  cublasHandle_t blas = nullptr;
   DBuf<double> out;
   // leaves grouped by level (P2M / L2P operators are per level except for Laplace)
   std::vector<int> leaf_level_off;
@@ -1171,6 +1153,7 @@ struct Workspace {
   std::vector<cudaEvent_t> m2l_ev;  // 4 per M2L group
   bool ev_ok = false;
   ~Workspace() {
+    if (blas) cublasDestroy(blas);
     for (auto h : fwd) cufftDestroy(h);
     for (auto h : bwd) cufftDestroy(h);
     if (ev_ok) {
@@ -1195,8 +1178,6 @@ void upload_rows(GemmRows& g, const std::vector<int64_t>& a, const std::vector<i
   g.M = (int)a.size();
   g.a.upload(a, s);
   g.c.upload(c, s);
-  std::vector<float> f(al.begin(), al.end());
-  g.al32.upload(f, s);
   g.al64.upload(al, s);
 }
 
@@ -1217,6 +1198,8 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   W.chk.alloc((size_t)std::max(t.nleafs, 1) * n * W.vsz);
   W.ybuf.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
   W.eq.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
+  W.xbuf.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
+  XCUBLAS2(cublasCreate(&W.blas));
   W.out.alloc((size_t)t.ntrg * 4 * (cplx ? 2 : 1));
   // leaf rows grouped by level: P2M (chk[pos] -> up[node]) and L2P (dn[node] -> eq[pos])
   const bool lap = f.kernel == XFMM_LAPLACE;
@@ -1264,6 +1247,12 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
       }
     upload_rows<double>(W.m2m[l], ma, mc, one, s);
     upload_rows<double>(W.l2l[l], la, lc, one, s);
+  }
+  {
+    int maxp = 1;
+    for (int l = 0; l <= t.depth; l++) maxp = std::max(maxp, W.m2m[l].M);
+    W.wA.alloc((size_t)maxp * 8 * n * W.vsz);
+    W.wC.alloc((size_t)maxp * 8 * n * W.vsz);
   }
   // M2L buffers and FFT plans
   const int ng = (int)t.m2l_src_off.size() - 1;
@@ -1450,6 +1439,9 @@ struct Engine {
       XLAUNCH();
       ws.launches++;
       W* up = (W*)ws.up.p;
+      V64* X = (V64*)ws.xbuf.p;
+      V64* Y = (V64*)ws.ybuf.p;
+      XCUBLAS2(cublasSetStream(ws.blas, s));
       for (int l = 0; l <= t.depth; l++) {
         if (KER == K_LAPLACE && l > 0) break;
         const int r0 = ws.leaf_level_off[l], r1 = ws.leaf_level_off[l + 1];
@@ -1457,21 +1449,35 @@ struct Engine {
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
         const Ops<W, V64> o = ops_of<W, V64>(f, l);
-        ws.launches++;
-        gemm_rows<W, V64, V64>(m, n, n, (const W*)ws.chk.p, ws.p2m1.a.p + off, o.p2m1, (V64*)ws.ybuf.p,
-                               ws.p2m1.c.p + off, nullptr, 0, s);
-        ws.launches++;
-        gemm_rows<V64, V64, W>(m, n, n, (const V64*)ws.ybuf.p, ws.p2m2.a.p + off, o.p2m2, up, ws.p2m2.c.p + off,
-                               alpha_of<double>(ws.p2m2) + off, 0, s);
+        // rows of this leaf level, contiguous in FP64; e = (V S+) (U^H c) in two FP64 GEMMs; scaled scatter
+        const int64_t tot = (int64_t)m * n;
+        k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.chk.p, ws.p2m1.a.p + off, nullptr,
+                                                            X + (int64_t)off * n);
+        XLAUNCH();
+        gemm_rm(ws.blas, m, n, n, X + (int64_t)off * n, o.p2m1, Y + (int64_t)off * n);
+        gemm_rm(ws.blas, m, n, n, Y + (int64_t)off * n, o.p2m2, X + (int64_t)off * n);
+        k_rows_scatter<V64, W><<<rows_grid(tot), 256, 0, s>>>(m, n, X + (int64_t)off * n, ws.p2m2.c.p + off,
+                                                             alpha_of<double>(ws.p2m2) + off, up, 0);
+        XLAUNCH();
+        ws.launches += 2;
       }
     }
     XCUDA(cudaEventRecord(ws.ev[1], s));
-    // M2M: deepest parents first (post-order)
+    // M2M: deepest parents first (post-order); per level the parents' 8 children rows (contiguous per
+    // parent) gathered, one GEMM with the [8n][n] operator, the results scattered to the parents
+    XCUBLAS2(cublasSetStream(ws.blas, s));
     for (int l = t.depth - 1; l >= 0; l--) {
       const GemmRows& g = ws.m2m[l];
-      ws.launches++;
-        gemm_rows<W, W, W>(g.M, n, 8 * n, (const W*)ws.up.p, g.a.p, ops_of<W, V64>(f, l).m2m, (W*)ws.up.p, g.c.p,
-                           nullptr, 0, s);
+      if (g.M <= 0) continue;
+      const int64_t tot = (int64_t)g.M * 8 * n;
+      k_rows_gather<W, W><<<rows_grid(tot), 256, 0, s>>>(g.M, 8 * n, (const W*)ws.up.p, g.a.p, nullptr,
+                                                        (W*)ws.wA.p);
+      XLAUNCH();
+      gemm_rm(ws.blas, g.M, n, 8 * n, (const W*)ws.wA.p, ops_of<W, V64>(f, l).m2m, (W*)ws.wC.p);
+      k_rows_scatter<W, W><<<rows_grid((int64_t)g.M * n), 256, 0, s>>>(g.M, n, (const W*)ws.wC.p, g.c.p, nullptr,
+                                                                      (W*)ws.up.p, 0);
+      XLAUNCH();
+      ws.launches += 2;
     }
     XCUDA(cudaEventRecord(ws.ev[2], s));
   }
@@ -1582,16 +1588,27 @@ struct Engine {
     // M2L
     if (t.n_m2l_trg) m2l(f, t, ws, s);
     XCUDA(cudaEventRecord(ws.ev[4], s));
-    // L2L: shallowest parents first (pre-order)
+    // L2L: shallowest parents first (pre-order); per level the parents' rows gathered, one GEMM with the
+    // [n][8n] operator, the results added to the 8 children rows (contiguous per parent)
+    XCUBLAS2(cublasSetStream(ws.blas, s));
     for (int l = 0; l < t.depth; l++) {
       const GemmRows& g = ws.l2l[l];
-      ws.launches++;
-        gemm_rows<W, W, W>(g.M, 8 * n, n, (const W*)ws.dn.p, g.a.p, ops_of<W, V64>(f, l).l2l, (W*)ws.dn.p, g.c.p,
-                           nullptr, 1, s);
+      if (g.M <= 0) continue;
+      k_rows_gather<W, W><<<rows_grid((int64_t)g.M * n), 256, 0, s>>>(g.M, n, (const W*)ws.dn.p, g.a.p, nullptr,
+                                                                      (W*)ws.wA.p);
+      XLAUNCH();
+      gemm_rm(ws.blas, g.M, 8 * n, n, (const W*)ws.wA.p, ops_of<W, V64>(f, l).l2l, (W*)ws.wC.p);
+      k_rows_scatter<W, W><<<rows_grid((int64_t)g.M * 8 * n), 256, 0, s>>>(g.M, 8 * n, (const W*)ws.wC.p, g.c.p,
+                                                                          nullptr, (W*)ws.dn.p, 1);
+      XLAUNCH();
+      ws.launches += 2;
     }
     XCUDA(cudaEventRecord(ws.ev[5], s));
-    // L2P part 1: downward check -> equivalent (DC2E) per leaf level
+    // L2P part 1: downward check -> equivalent (DC2E) per leaf level: leaf rows gathered in FP64 with
+    // their scale, e = conj(U) S+ (conj(VH) c) in two FP64 GEMMs, scattered to the leaf positions
     if (t.nleafs) {
+      V64* X = (V64*)ws.xbuf.p;
+      V64* Y = (V64*)ws.ybuf.p;
       for (int l = 0; l <= t.depth; l++) {
         if (KER == K_LAPLACE && l > 0) break;
         const int r0 = ws.leaf_level_off[l], r1 = ws.leaf_level_off[l + 1];
@@ -1599,12 +1616,16 @@ struct Engine {
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
         const Ops<W, V64> o = ops_of<W, V64>(f, l);
-        ws.launches++;
-        gemm_rows<W, V64, V64>(m, n, n, (const W*)ws.dn.p, ws.l2p1.a.p + off, o.l2p1, (V64*)ws.ybuf.p,
-                               ws.l2p1.c.p + off, nullptr, 0, s);
-        ws.launches++;
-        gemm_rows<V64, V64, V64>(m, n, n, (const V64*)ws.ybuf.p, ws.l2p2.a.p + off, o.l2p2, (V64*)ws.eq.p,
-                                 ws.l2p2.c.p + off, alpha_of<double>(ws.l2p2) + off, 0, s);
+        const int64_t tot = (int64_t)m * n;
+        k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.dn.p, ws.l2p1.a.p + off,
+                                                            alpha_of<double>(ws.l2p2) + off, X + (int64_t)off * n);
+        XLAUNCH();
+        gemm_rm(ws.blas, m, n, n, X + (int64_t)off * n, o.l2p1, Y + (int64_t)off * n);
+        gemm_rm(ws.blas, m, n, n, Y + (int64_t)off * n, o.l2p2, X + (int64_t)off * n);
+        k_rows_scatter<V64, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, X + (int64_t)off * n, ws.l2p2.c.p + off,
+                                                               nullptr, (V64*)ws.eq.p, 0);
+        XLAUNCH();
+        ws.launches += 2;
       }
     }
     XCUDA(cudaEventRecord(ws.ev[6], s));
