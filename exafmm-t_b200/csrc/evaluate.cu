@@ -18,6 +18,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 
 #include "kernels.cuh"
@@ -1074,6 +1075,205 @@ __global__ void __launch_bounds__(HADD_NT, 2)
   }
 }
 
+// ---------------------------------------------------------------- M2L transforms of the real kernels
+// The convolution grid of one child is n1^3 (n1 = 2p), index a + b n1 + c n1^2 (a fastest).  The upward
+// equivalent values occupy the corner [0, p)^3 (geometry.h:101-134, up), the downward check values are
+// read from the corner [p, 2p)^3 (down).  The forward transform is the real-to-half-complex DFT of the
+// grid (factor e^{-2 pi i k n / n1}, unnormalised, frequency f = (kc n1 + kb)(p + 1) + ka), the backward
+// one the half-complex-to-real DFT (factor e^{+...}, unnormalised): the transforms of the reference's
+// FFTW plans (fmm_scale_invariant.h:560-646).  Because only a p^3 corner of each input is non-zero and
+// only a p^3 corner of each output is used, both are computed as three passes of direct sums, one axis
+// at a time, in shared memory: no grid is materialised, and each spectrum value is written once by
+// k_m2l_fwd and read once by k_m2l_bwd, in the Hadamard product's [frequency][node][child] layout.
+// A CTA handles FT_CPB(R) children of one node: their spectrum values of one frequency are contiguous.
+// The expansion order P is a template parameter (2 <= P <= FT_PMAX), so every loop unrolls and each
+// DFT factor w^(jk mod n1) is a register chosen at compile time.
+constexpr int FT_NT = 256;
+constexpr int FT_PMAX = 10;
+template <class R> struct FtCpb;
+template <> struct FtCpb<float> { static constexpr int v = 8; };   // 64-byte chunks of float2
+template <> struct FtCpb<double> { static constexpr int v = 4; };  // 64-byte chunks of double2
+template <class R> struct FtMinB;
+template <> struct FtMinB<float> { static constexpr int v = 2; };
+template <> struct FtMinB<double> { static constexpr int v = 1; };
+
+// calls fn(std::integral_constant<int, p>) for 2 <= p <= FT_PMAX
+template <class F>
+void ft_dispatch(int p, F&& fn) {
+  switch (p) {
+    case 2: fn(std::integral_constant<int, 2>()); break;
+    case 3: fn(std::integral_constant<int, 3>()); break;
+    case 4: fn(std::integral_constant<int, 4>()); break;
+    case 5: fn(std::integral_constant<int, 5>()); break;
+    case 6: fn(std::integral_constant<int, 6>()); break;
+    case 7: fn(std::integral_constant<int, 7>()); break;
+    case 8: fn(std::integral_constant<int, 8>()); break;
+    case 9: fn(std::integral_constant<int, 9>()); break;
+    case 10: fn(std::integral_constant<int, 10>()); break;
+    default: throw Error(XFMM_ERR_UNSUPPORTED, "M2L transform kernels cover 2 <= p <= 10");
+  }
+}
+
+template <class R>
+size_t ft_fwd_smem(int p) {
+  const int n1 = 2 * p, h = p + 1, cpb = FtCpb<R>::v;
+  return sizeof(typename C2<R>::type) * ((size_t)cpb * p * p * h + (size_t)cpb * p * n1 * h);
+}
+template <class R>
+size_t ft_bwd_smem(int p) { return ft_fwd_smem<R>(p); }
+
+// w[m] = e^{sign 2 pi i m / n1} from the (cos, sin) table
+template <class CT, int N>
+__device__ __forceinline__ void ft_load_w(const double* __restrict__ tw, double sign, CT (&w)[N]) {
+#pragma unroll
+  for (int m = 0; m < N; m++) {
+    w[m].x = (decltype(w[m].x))tw[2 * m];
+    w[m].y = (decltype(w[m].x))(sign * tw[2 * m + 1]);
+  }
+}
+
+// spec[(f*ns + s)*8 + child] = forward DFT of child `child` of source node src[s]
+template <class R, int P>
+__global__ void __launch_bounds__(FT_NT, FtMinB<R>::v)
+    k_m2l_fwd(const int* __restrict__ src, int ns, const int* __restrict__ child0, const R* __restrict__ up, int nsurf,
+              const int* __restrict__ map_up, const double* __restrict__ tw, typename C2<R>::type* __restrict__ spec) {
+  using CT = typename C2<R>::type;
+  constexpr int CPB = FtCpb<R>::v, N = 2 * P, H = P + 1, NC = N * H;
+  const int s = blockIdx.x, ch0 = blockIdx.y * CPB, tid = threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* sA = reinterpret_cast<CT*>(smem_raw);  // [CPB][c < P][b < P][ka < H]
+  CT* sB = sA + CPB * P * P * H;             // [CPB][c < P][kb < N][ka < H]
+  R* sx = reinterpret_cast<R*>(sB);          // [CPB][c][b][a < P], dead before sB is written
+  CT w[N];
+  ft_load_w(tw, -1.0, w);
+  for (int e = tid; e < CPB * P * P * P; e += FT_NT) sx[e] = (R)0;
+  __syncthreads();
+  const int64_t node0 = (int64_t)child0[src[s]] + ch0;
+  for (int e = tid; e < CPB * nsurf; e += FT_NT) {
+    const int ch = e / nsurf, k = e - ch * nsurf, g = map_up[k];
+    const int a = g % N, b = (g / N) % N, c = g / (N * N);
+    sx[((ch * P + c) * P + b) * P + a] = up[(node0 + ch) * nsurf + k];
+  }
+  __syncthreads();
+  // pass 1, along a (real input), one row (ch, c, b) per task: sA[row][ka] = sum_a x[row][a] w^{ka a}
+  for (int row = tid; row < CPB * P * P; row += FT_NT) {
+    R x[P];
+#pragma unroll
+    for (int a = 0; a < P; a++) x[a] = sx[row * P + a];
+#pragma unroll
+    for (int ka = 0; ka < H; ka++) {
+      R re = 0, im = 0;
+#pragma unroll
+      for (int a = 0; a < P; a++) {
+        re += x[a] * w[(ka * a) % N].x;
+        im += x[a] * w[(ka * a) % N].y;
+      }
+      sA[row * H + ka] = CT{re, im};
+    }
+  }
+  __syncthreads();
+  // pass 2, along b, one column (ch, c, ka) per task: sB[(cc N + kb) H + ka] = sum_b sA[(cc P + b) H + ka] w^{kb b}
+  for (int e = tid; e < CPB * P * H; e += FT_NT) {
+    const int ka = e % H, cc = e / H;
+    CT v[P];
+#pragma unroll
+    for (int b = 0; b < P; b++) v[b] = sA[(cc * P + b) * H + ka];
+#pragma unroll
+    for (int kb = 0; kb < N; kb++) {
+      CT acc = v[0];
+#pragma unroll
+      for (int b = 1; b < P; b++) vfma(acc, v[b], w[(kb * b) % N]);
+      sB[(cc * N + kb) * H + ka] = acc;
+    }
+  }
+  __syncthreads();
+  // pass 3, along c, one column (ch, kb, ka) per task: spec[f = (kc N + kb) H + ka][s][ch0 + ch]
+  for (int e = tid; e < NC * CPB; e += FT_NT) {
+    const int ch = e % CPB, col = e / CPB;
+    CT v[P];
+#pragma unroll
+    for (int c = 0; c < P; c++) v[c] = sB[(ch * P + c) * NC + col];
+    CT* o = spec + ((int64_t)col * ns + s) * 8 + ch0 + ch;
+    const int64_t fstride = (int64_t)NC * ns * 8;
+#pragma unroll
+    for (int kc = 0; kc < N; kc++) {
+      CT acc = v[0];
+#pragma unroll
+      for (int c = 1; c < P; c++) vfma(acc, v[c], w[(kc * c) % N]);
+      o[kc * fstride] = acc;
+    }
+  }
+}
+
+// dn[child of target trg[t]][k] += scale[t] * backward DFT of spec[.][t][child] at map_dn[k]
+template <class R, int P>
+__global__ void __launch_bounds__(FT_NT, FtMinB<R>::v)
+    k_m2l_bwd(const int* __restrict__ trg, int nt, const int* __restrict__ child0,
+              const typename C2<R>::type* __restrict__ spec, int nsurf, const int* __restrict__ map_dn,
+              const double* __restrict__ tw, const R* __restrict__ scale, R* __restrict__ dn) {
+  using CT = typename C2<R>::type;
+  constexpr int CPB = FtCpb<R>::v, N = 2 * P, H = P + 1, NC = N * H;
+  const int t = blockIdx.x, ch0 = blockIdx.y * CPB, tid = threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* sZ1 = reinterpret_cast<CT*>(smem_raw);  // [CPB][c' < P][kb < N][ka < H]
+  CT* sZ2 = sZ1 + CPB * P * NC;               // [CPB][c' < P][b' < P][ka < H]
+  __shared__ CT sw[2 * FT_PMAX];
+  CT w[N];
+  ft_load_w(tw, 1.0, w);
+  if (tid < N) sw[tid] = CT{(R)tw[2 * tid], (R)tw[2 * tid + 1]};
+  // pass A, along kc, to the outputs c = P + c', one column (ch, kb, ka) per task
+  for (int e = tid; e < NC * CPB; e += FT_NT) {
+    const int ch = e % CPB, col = e / CPB;
+    const CT* y = spec + ((int64_t)col * nt + t) * 8 + ch0 + ch;
+    const int64_t fstride = (int64_t)NC * nt * 8;
+    CT v[N];
+#pragma unroll
+    for (int kc = 0; kc < N; kc++) v[kc] = y[kc * fstride];
+#pragma unroll
+    for (int cc = 0; cc < P; cc++) {
+      CT acc = v[0];
+#pragma unroll
+      for (int kc = 1; kc < N; kc++) vfma(acc, v[kc], w[(kc * (P + cc)) % N]);
+      sZ1[(ch * P + cc) * NC + col] = acc;
+    }
+  }
+  __syncthreads();
+  // pass B, along kb, to the outputs b = P + b', one column (ch, c', ka) per task
+  for (int e = tid; e < CPB * P * H; e += FT_NT) {
+    const int ka = e % H, cc = e / H;
+    CT v[N];
+#pragma unroll
+    for (int kb = 0; kb < N; kb++) v[kb] = sZ1[(cc * N + kb) * H + ka];
+#pragma unroll
+    for (int bb = 0; bb < P; bb++) {
+      CT acc = v[0];
+#pragma unroll
+      for (int kb = 1; kb < N; kb++) vfma(acc, v[kb], w[(kb * (P + bb)) % N]);
+      sZ2[(cc * P + bb) * H + ka] = acc;
+    }
+  }
+  __syncthreads();
+  // pass C, along ka (half-complex to real: weight 2 except at ka = 0 and ka = N/2), at the check points;
+  // the factor index (ka a mod N) depends on the point, so the factors are read from shared memory
+  const int64_t node0 = (int64_t)child0[trg[t]] + ch0;
+  const R sc = scale[t];
+  for (int e = tid; e < CPB * nsurf; e += FT_NT) {
+    const int ch = e / nsurf, k = e - ch * nsurf, g = map_dn[k];
+    const int a = g % N, b = g / N % N - P, c = g / (N * N) - P;
+    const CT* z = sZ2 + ((ch * P + c) * P + b) * H;
+    R y = z[0].x;
+    for (int ka = 1, m = a; ka < H; ka++) {
+      const R wgt = 2 * ka == N ? (R)1 : (R)2;
+      const CT ww = sw[m];
+      y += wgt * (z[ka].x * ww.x - z[ka].y * ww.y);
+      m += a;
+      if (m >= N) m -= N;
+    }
+    R* d = dn + (node0 + ch) * nsurf + k;
+    *d += sc * y;
+  }
+}
+
 // dn[child c of target t][k] += scale[t] * grid[(t*8 + c)*nconv + map_dn[k]]   (fmm_scale_invariant.h:639-643)
 template <class W, class RB>
 __global__ void k_m2l_gather_dn(const int* __restrict__ trg, int ntrg, const int* __restrict__ child0,
@@ -1148,6 +1348,9 @@ struct Workspace {
   std::vector<int64_t> hadd_tab0, hadd_row0;
   std::vector<int> hadd_ld;
   size_t hadamard_smem = 0;
+  // M2L transforms: own pruned DFT kernels (real kernels, shared memory permitting) or cuFFT on the grid
+  bool fused = false;
+  size_t ft_fwd_smem = 0, ft_bwd_smem = 0;
   int64_t launches = 0;  // kernels of this library launched by the last evaluate
   cudaEvent_t ev[8] = {};
   std::vector<cudaEvent_t> m2l_ev;  // 4 per M2L group
@@ -1262,14 +1465,19 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
     maxn = std::max(maxn, t.m2l_trg_off[g + 1] - t.m2l_trg_off[g]);
   }
   const size_t rsz = f.mixed() ? 4 : 8;  // real scalar size
-  const size_t grid_vals = (size_t)maxn * 8 * f.nconv;
-  W.grid.alloc(grid_vals * rsz * (cplx ? 2 : 1));
+  {
+    constexpr size_t kMaxSmem = 227 * 1024;
+    const size_t fw = f.mixed() ? ft_fwd_smem<float>(f.p) : ft_fwd_smem<double>(f.p);
+    const size_t bw = f.mixed() ? ft_bwd_smem<float>(f.p) : ft_bwd_smem<double>(f.p);
+    W.fused = !cplx && f.p <= FT_PMAX && fw <= kMaxSmem && bw <= kMaxSmem;
+  }
   W.specA.alloc((size_t)maxn * 8 * f.nfreq * 2 * rsz);
   W.specB.alloc((size_t)maxn * 8 * f.nfreq * 2 * rsz);
   int dims[3] = {f.n1, f.n1, f.n1};
   cufftType tf = cplx ? (f.mixed() ? CUFFT_C2C : CUFFT_Z2Z) : (f.mixed() ? CUFFT_R2C : CUFFT_D2Z);
   cufftType tb = cplx ? (f.mixed() ? CUFFT_C2C : CUFFT_Z2Z) : (f.mixed() ? CUFFT_C2R : CUFFT_Z2D);
-  for (int g = 0; g < ng; g++) {
+  if (!W.fused) W.grid.alloc((size_t)maxn * 8 * f.nconv * rsz * (cplx ? 2 : 1));
+  for (int g = 0; g < ng && !W.fused; g++) {
     const int ns = t.m2l_src_off[g + 1] - t.m2l_src_off[g], nt = t.m2l_trg_off[g + 1] - t.m2l_trg_off[g];
     cufftHandle hf = 0, hb = 0;
     if (ns > 0) {
@@ -1494,14 +1702,33 @@ struct Engine {
       const int tab_level = KER == K_LAPLACE ? 0 : g + 1;
       const CT* T = (const CT*)f.ops[tab_level].m2l_T.p;
       XCUDA(cudaEventRecord(ev[0], s));
-      // upward equivalent FFT (fmm_scale_invariant.h:560-604)
-      k_m2l_grid_up<W><<<std::min<int64_t>(nblk((int64_t)ns * 8 * nconv), 148 * 32), 256, 0, s>>>(
-          src, ns, t.child0.p, (const W*)ws.up.p, n, f.conv_to_surf_up.p, nconv, (W*)ws.grid.p);
-      XLAUNCH();
-      ws.launches++;
-      exec_fwd(ws.fwd[g], ws.grid.p, ws.specA.p);
-      ws.launches++;
-      transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, (int64_t)ns * 8, nfreq, s);  // -> [f][s][c]
+      // upward equivalent DFT (fmm_scale_invariant.h:560-604) -> specB [f][s][c]
+      if constexpr (KER != K_HELMHOLTZ) {
+        if (ws.fused) {
+          ft_dispatch(f.p, [&](auto pc) {
+            constexpr int PP = decltype(pc)::value;
+            const size_t smem = ft_fwd_smem<R>(PP);
+            if (ws.ft_fwd_smem < smem) {
+              XCUDA(cudaFuncSetAttribute(k_m2l_fwd<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+              ws.ft_fwd_smem = smem;
+            }
+            k_m2l_fwd<R, PP><<<dim3(ns, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
+                src, ns, t.child0.p, (const R*)ws.up.p, n, f.map_up.p, f.dft_tw.p, (CT*)ws.specB.p);
+          });
+          XLAUNCH();
+          ws.launches++;
+        }
+      }
+      if (!ws.fused) {
+        k_m2l_grid_up<W><<<std::min<int64_t>(nblk((int64_t)ns * 8 * nconv), 148 * 32), 256, 0, s>>>(
+            src, ns, t.child0.p, (const W*)ws.up.p, n, f.conv_to_surf_up.p, nconv, (W*)ws.grid.p);
+        XLAUNCH();
+        ws.launches++;
+        XCUFFT2(cufftSetStream(ws.fwd[g], s));
+        exec_fwd(ws.fwd[g], ws.grid.p, ws.specA.p);
+        ws.launches++;
+        transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, (int64_t)ns * 8, nfreq, s);  // -> [f][s][c]
+      }
       XCUDA(cudaEventRecord(ev[1], s));
       // Hadamard product
       const int ntiles = ws.had_tile0[g + 1] - ws.had_tile0[g];
@@ -1541,15 +1768,35 @@ struct Engine {
         ws.launches++;
       }
       XCUDA(cudaEventRecord(ev[2], s));
-      // inverse FFT to downward check potentials (fmm_scale_invariant.h:606-646)
-      ws.launches++;
-      transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, nfreq, (int64_t)nt * 8, s);  // -> [t][c][f]
-      exec_bwd(ws.bwd[g], ws.specB.p, ws.grid.p);
-      k_m2l_gather_dn<W, R><<<std::min<int64_t>(nblk((int64_t)nt * 8 * n), 148 * 32), 256, 0, s>>>(
-          trg, nt, t.child0.p, (const W*)ws.grid.p, nconv, f.map_dn.p, n,
-          m2l_scale_of<R>(t) + t.m2l_trg_off[g], (W*)ws.dn.p);
-      XLAUNCH();
-      ws.launches++;
+      // inverse DFT of specA [f][t][c] to the downward check potentials (fmm_scale_invariant.h:606-646)
+      if constexpr (KER != K_HELMHOLTZ) {
+        if (ws.fused) {
+          ft_dispatch(f.p, [&](auto pc) {
+            constexpr int PP = decltype(pc)::value;
+            const size_t smem = ft_bwd_smem<R>(PP);
+            if (ws.ft_bwd_smem < smem) {
+              XCUDA(cudaFuncSetAttribute(k_m2l_bwd<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+              ws.ft_bwd_smem = smem;
+            }
+            k_m2l_bwd<R, PP><<<dim3(nt, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
+                trg, nt, t.child0.p, (const CT*)ws.specA.p, n, f.map_dn.p, f.dft_tw.p,
+                m2l_scale_of<R>(t) + t.m2l_trg_off[g], (R*)ws.dn.p);
+          });
+          XLAUNCH();
+          ws.launches++;
+        }
+      }
+      if (!ws.fused) {
+        ws.launches++;
+        transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, nfreq, (int64_t)nt * 8, s);  // -> [t][c][f]
+        XCUFFT2(cufftSetStream(ws.bwd[g], s));
+        exec_bwd(ws.bwd[g], ws.specB.p, ws.grid.p);
+        k_m2l_gather_dn<W, R><<<std::min<int64_t>(nblk((int64_t)nt * 8 * n), 148 * 32), 256, 0, s>>>(
+            trg, nt, t.child0.p, (const W*)ws.grid.p, nconv, f.map_dn.p, n,
+            m2l_scale_of<R>(t) + t.m2l_trg_off[g], (W*)ws.dn.p);
+        XLAUNCH();
+        ws.launches += 2;
+      }
       XCUDA(cudaEventRecord(ev[3], s));
     }
   }

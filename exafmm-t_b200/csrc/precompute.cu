@@ -281,6 +281,17 @@ void precompute(Fmm& f, int depth, cudaStream_t s) {
   std::vector<int> inv(nconv, -1);
   for (int k = 0; k < n; k++) inv[mup[k]] = k;
   f.conv_to_surf_up.upload(inv, s);
+  {
+    // e^{2 pi i m / n1} for m < n1, as (cos, sin) pairs: the DFT factors of the M2L transforms
+    const int n1 = 2 * p;
+    std::vector<double> tw(2 * n1);
+    for (int m = 0; m < n1; m++) {
+      const double a = 2.0 * 3.14159265358979323846 * m / n1;
+      tw[2 * m] = std::cos(a);
+      tw[2 * m + 1] = std::sin(a);
+    }
+    f.dft_tw.upload(tw, s);
+  }
   std::vector<int> imap = m2l_index_map();
   DBuf<int> d_imap;
   d_imap.upload(imap, s);

@@ -175,6 +175,7 @@ struct Fmm {
   DBuf<double> surf_base;             // [nsurf][3] unit surface (geometry.h:21-54 before scaling)
   DBuf<int> map_up, map_dn;           // surface index -> conv-grid index (geometry.h:101-134)
   DBuf<int> conv_to_surf_up;          // conv-grid index -> surface index or -1
+  DBuf<double> dft_tw;                // [n1] (cos, sin)(2 pi m / n1): factors of the M2L transforms
   std::vector<double> h_surf_base;
   double stage_ms[11] = {0};
   bool is_complex() const { return kernel == XFMM_HELMHOLTZ; }
