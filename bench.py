@@ -192,27 +192,50 @@ def accuracy(outs, x, q):
     return {k: dict(zip(("potential", "gradient"), orc.rel_l2(v[samp], ex))) for k, v in outs.items()}
 
 
+# DRAM bytes per launch of the dominant kernel from an ncu capture of this workload (summarised under
+# profiles/, with the command); None until captured.
+NEAR_TRAFFIC_BYTES = None
+
+
 def roofline(r, peaks, src):
-    """Dominant kernels: target evaluation (FP32 SIMT FLOP/s) and the M2L Hadamard (HBM bytes)."""
+    """Per-kernel rooflines from the device stage times of the timed path.
+
+    near  P2P (k_near_lap_f2): FP32 SIMT FLOP/s, 28 flops per pair (the reference's count,
+          laplace.h:163) against the nominal FP32 SIMT peak (148 SMs x 128 lanes x 2 at the sampled clock)
+    m2l   forward transform + Hadamard + backward transform: algorithmic HBM bytes against measured copy
+          bandwidth (spectra written once, read by the Hadamard, products written once, read once)
+    trans P2M/L2P pseudo-inverse (FP64) and M2M/L2L (FP32) GEMM FLOP/s
+    """
     info, st = r["info"], r["stages"]
-    n = 8  # children per node
+    nsurf = 6 * (P - 1) ** 2 + 2
     nfreq = (2 * P) ** 2 * (P + 1)
-    # M2L Hadamard algorithmic bytes: spectra in (sources) + out (targets) + 26 tables, complex64
-    had_bytes = (info["n_m2l_src"] + info["nnonleafs"]) * n * nfreq * 8 + 26 * nfreq * 64 * 8
-    had_ms = st["M2L_hadamard"]
     sm_mhz = r["clocks"].get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s, FMA = 2 flops
-    pairs = info["p2p_pairs"] + info["m2p_pairs"] + info["l2p_pairs"]
-    eval_tflops = pairs * FLOPS_PER_P2P_PAIR / (st["P2P_M2P_L2P"] * 1e-3) / 1e12
-    had = {"bound": "hbm", "achieved": had_bytes / (had_ms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
-           "unit": "GB/s", "frac": None, "traffic": None, "kernel": "k_hadamard (M2L)",
-           "algorithmic_bytes_per_launch": had_bytes, "ms_per_launch": had_ms, "peak_source": src}
-    had["frac"] = had["achieved"] / had["peak"]
-    ev = {"bound": "fp32-simt", "achieved": eval_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
-          "frac": eval_tflops / fp32_peak, "kernel": "k_eval (P2P+M2P+L2P)", "pairs_per_launch": pairs,
-          "flops_per_pair": FLOPS_PER_P2P_PAIR, "ms_per_launch": st["P2P_M2P_L2P"],
-          "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 at the sampled SM clock"}
-    return had, ev
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    near_ms = st["P2P"]
+    near_tflops = info["p2p_pairs"] * FLOPS_PER_P2P_PAIR / (near_ms * 1e-3) / 1e12
+    near = {"bound": "fp32-simt", "achieved": near_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": near_tflops / fp32_peak, "traffic": NEAR_TRAFFIC_BYTES, "kernel": "k_near_lap_f2 (P2P)",
+            "pairs_per_launch": info["p2p_pairs"], "flops_per_pair": FLOPS_PER_P2P_PAIR, "ms_per_launch": near_ms,
+            "peak_source": "nominal FP32 SIMT: 148 SM x 128 lanes x 2 flops at the sampled SM clock"}
+    ns, nt = info["n_m2l_src"], info["nnonleafs"]
+    spec = nfreq * 8 * 8  # complex64 spectrum of one node's 8 children
+    m2l_bytes = (ns * 8 * nsurf * 4 + ns * spec  # forward: up in, spectra out
+                 + ns * spec + nt * spec + 26 * nfreq * 64 * 8  # Hadamard: spectra in, products out, tables
+                 + nt * spec + nt * 8 * nsurf * 4 * 2)  # backward: products in, dn read-modify-write
+    m2l_ms = st["M2L_fft"] + st["M2L_hadamard"] + st["M2L_ifft"]
+    m2l = {"bound": "hbm", "achieved": m2l_bytes / (m2l_ms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+           "kernel": "k_m2l_fwd + k_hadamard_d/k_hadamard_r + k_m2l_bwd (M2L)", "algorithmic_bytes": m2l_bytes,
+           "ms": m2l_ms, "ms_transforms": st["M2L_fft"] + st["M2L_ifft"], "ms_hadamard": st["M2L_hadamard"],
+           "peak_source": src}
+    m2l["frac"] = m2l["achieved"] / m2l["peak"]
+    nl = info["nleafs"]
+    pinv_flops = 4 * 2.0 * nl * nsurf * nsurf  # two FP64 GEMMs each for P2M and L2P
+    tr_flops = 2 * 2.0 * (info["nnonleafs"]) * nsurf * 8 * nsurf  # M2M + L2L
+    trans = {"pinv_fp64_tflops": pinv_flops / ((st["P2M"] + st["L2P_dc2e"]) * 1e-3) / 1e12,
+             "m2m_l2l_fp32_tflops": tr_flops / ((st["M2M"] + st["L2L"]) * 1e-3) / 1e12,
+             "note": "library GEMMs (FP64 and FP32, not tensor-core TF32: the FP32 translations keep the 1e-6 error "
+                     "budget); stage times include the row gather/scatter kernels and, for P2M, the check potentials"}
+    return near, m2l, trans
 
 
 def cpu_baseline(n_sample, steps=1):
@@ -281,7 +304,7 @@ def main():
     acc = accuracy(outs, x, q)
     peaks, src = measured_peaks()
     m = res["mixed"]
-    had, ev = roofline(m, peaks, src)
+    near, m2l, trans = roofline(m, peaks, src)
     n = args.n
     value = n * world / (m["ms"] * 1e-3) / 1e6
     line = {
@@ -300,8 +323,9 @@ def main():
                 "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 4 * 8,
                 "note": "exafmm.laplace.update_charges + evaluate on pinned host arrays (C ABI host path), wall clock incl. copies"},
         "gpu_launches": int(m["stages"]["launches"]) * args.steps,
-        "roofline": had,
-        "roofline_eval": ev,
+        "roofline": near,
+        "roofline_m2l": m2l,
+        "translations": trans,
         "stages_ms": {k: round(v, 3) for k, v in m["stages"].items() if k != "launches"},
         "setup_s": m["setup_s"],
     }

@@ -292,10 +292,10 @@ xfmm_status xfmm_tree_dump(const xfmm_tree* tree, double* geo, uint64_t* key, in
   });
 }
 
-xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms12) {
+xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms14) {
   return guarded([&] {
-    XREQUIRE(fmm && tree && ms12, XFMM_ERR_ARG, "null argument");
-    xfmm::stage_times(fmm->f, tree->t, ms12);
+    XREQUIRE(fmm && tree && ms14, XFMM_ERR_ARG, "null argument");
+    xfmm::stage_times(fmm->f, tree->t, ms14);
   });
 }
 

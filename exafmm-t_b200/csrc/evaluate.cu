@@ -1352,7 +1352,7 @@ struct Workspace {
   bool fused = false;
   size_t ft_fwd_smem = 0, ft_bwd_smem = 0;
   int64_t launches = 0;  // kernels of this library launched by the last evaluate
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[9] = {};
   std::vector<cudaEvent_t> m2l_ev;  // 4 per M2L group
   bool ev_ok = false;
   ~Workspace() {
@@ -1892,11 +1892,14 @@ struct Engine {
         k_near<KER, R><<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
       XLAUNCH();
       ws.launches++;
+      XCUDA(cudaEventRecord(ws.ev[8], s));
       a.do_near = 0;
       a.accumulate = 1;
       k_eval<KER, double, W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
       XLAUNCH();
       ws.launches++;
+    } else {
+      XCUDA(cudaEventRecord(ws.ev[8], s));
     }
     XCUDA(cudaEventRecord(ws.ev[7], s));
   }
@@ -1965,7 +1968,7 @@ void downward_pass(Fmm& f, Tree& t, cudaStream_t s) {
 
 // Device times of the last upward + downward pass (ms): 0 P2M, 1 M2M, 2 P2L, 3 M2L, 4 L2L,
 // 5 L2P check->equivalent, 6 target evaluation (P2P + M2P + L2P), 7 total, 8-10 M2L FFT / Hadamard / iFFT.
-void stage_times(Fmm& f, Tree& t, double* ms11) {
+void stage_times(Fmm& f, Tree& t, double* ms14) {
   Workspace* ws = t.ws[f.precision];
   XREQUIRE(ws, XFMM_ERR_STATE, "no evaluate has run");
   XCUDA(cudaEventSynchronize(ws->ev[7]));
@@ -1974,19 +1977,21 @@ void stage_times(Fmm& f, Tree& t, double* ms11) {
     return cudaEventElapsedTime(&ms, a, b) == cudaSuccess ? (double)ms : 0.0;
   };
   const int pairs[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}, {0, 7}};
-  for (int i = 0; i < 8; i++) ms11[i] = el(ws->ev[pairs[i][0]], ws->ev[pairs[i][1]]);
-  ms11[8] = ms11[9] = ms11[10] = 0;
+  for (int i = 0; i < 8; i++) ms14[i] = el(ws->ev[pairs[i][0]], ws->ev[pairs[i][1]]);
+  ms14[8] = ms14[9] = ms14[10] = 0;
   const int ng = (int)ws->m2l_ev.size() / 4;
   for (int g = 0; g < ng; g++) {
     const int ns = t.m2l_src_off[g + 1] - t.m2l_src_off[g], nt = t.m2l_trg_off[g + 1] - t.m2l_trg_off[g];
     if (ns == 0 || nt == 0) continue;
     cudaEvent_t* e = ws->m2l_ev.data() + 4 * g;
-    ms11[8] += el(e[0], e[1]);
-    ms11[9] += el(e[1], e[2]);
-    ms11[10] += el(e[2], e[3]);
+    ms14[8] += el(e[0], e[1]);
+    ms14[9] += el(e[1], e[2]);
+    ms14[10] += el(e[2], e[3]);
   }
-  for (int i = 0; i < 11; i++) f.stage_ms[i] = ms11[i];
-  ms11[11] = (double)ws->launches;
+  for (int i = 0; i < 11; i++) f.stage_ms[i] = ms14[i];
+  ms14[11] = (double)ws->launches;
+  ms14[12] = el(ws->ev[6], ws->ev[8]);  // near field (P2P)
+  ms14[13] = el(ws->ev[8], ws->ev[7]);  // far field (M2P + L2P)
 }
 
 void get_values(Fmm& f, Tree& t, double* out_dev, cudaStream_t s) {

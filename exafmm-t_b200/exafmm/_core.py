@@ -104,11 +104,12 @@ class FmmBase:
 
     def stage_times(self, tree):
         """Device ms of the last evaluate on ``tree``: P2M, M2M, P2L, M2L, L2L, L2P(check->equiv),
-        P2P+M2P+L2P, total, and the M2L FFT / Hadamard / iFFT sub-stages."""
-        t = np.zeros(12)
+        P2P+M2P+L2P, total, the M2L forward-transform / Hadamard / backward-transform sub-stages, the
+        number of this library's kernel launches, and the near (P2P) / far (M2P+L2P) split."""
+        t = np.zeros(14)
         _lib.check(_lib.lib().xfmm_stage_times(self._h, tree._h, t.ctypes.data))
         names = ["P2M", "M2M", "P2L", "M2L", "L2L", "L2P_dc2e", "P2P_M2P_L2P", "total", "M2L_fft", "M2L_hadamard",
-                 "M2L_ifft", "launches"]
+                 "M2L_ifft", "launches", "P2P", "M2P_L2P"]
         return dict(zip(names, t.tolist()))
 
     def __del__(self):

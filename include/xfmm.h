@@ -107,9 +107,11 @@ xfmm_status xfmm_tree_dump(const xfmm_tree* tree, double* geo, uint64_t* key, in
                            int64_t* p2l_off, int32_t* p2l);
 /* Device times (ms, CUDA events) of the last upward + downward pass on this tree: P2M, M2M, P2L,
  * M2L, L2L, L2P check-to-equivalent, target evaluation (P2P + M2P + L2P), total; then the M2L
- * sub-stages FFT, Hadamard, iFFT; and the number of this library's kernel launches in the last
- * evaluate (12 doubles).  Waits for the last pass to finish. */
-xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms12);
+ * sub-stages forward transform, Hadamard, backward transform; the number of this library's kernel
+ * launches in the last evaluate (library GEMM and FFT launches not counted); then the target
+ * evaluation split into its near field (P2P) and far field (M2P + L2P) (14 doubles).  Waits for the
+ * last pass to finish. */
+xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms14);
 
 /* Direct near-field kernel over raw arrays: out (ntrg x 4) += potential and gradient
  * at trg from (src, q).  precision selects the FP64 or FP32 device kernel. */
