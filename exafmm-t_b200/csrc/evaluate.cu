@@ -582,14 +582,22 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
   }
 }
 
-__global__ void __launch_bounds__(128) k_near_lap_f2(NearArgs a) {
+#ifndef XFMM_NEARF2_MINB
+#define XFMM_NEARF2_MINB 1  // minimum resident blocks per SM requested from the register allocator
+#endif
+#ifndef XFMM_NEARF2_TPL
+#define XFMM_NEARF2_TPL 2  // largest number of targets per lane (2 or 4)
+#endif
+__global__ void __launch_bounds__(128, XFMM_NEARF2_MINB) k_near_lap_f2(NearArgs a) {
   __shared__ NearSmemF2 sm[4];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int w = blockIdx.x * 4 + wid;
   if (w >= a.n_eval) return;
   const int node = a.leafs[a.eval_leafs[w]];
-  if (a.ntrgs[node] <= 32) near_leaf_lap_f2<1>(a, node, lane, sm[wid]);
-  else near_leaf_lap_f2<2>(a, node, lane, sm[wid]);
+  const int T = a.ntrgs[node];
+  if (T <= 32) near_leaf_lap_f2<1>(a, node, lane, sm[wid]);
+  else if (T <= 64 || XFMM_NEARF2_TPL == 2) near_leaf_lap_f2<2>(a, node, lane, sm[wid]);
+  else near_leaf_lap_f2<XFMM_NEARF2_TPL>(a, node, lane, sm[wid]);
 }
 
 #ifndef XFMM_NEAR_MAXTPL
@@ -880,43 +888,26 @@ __global__ void __launch_bounds__(128 * HadKC<CT>::KC) k_hadamard(const CT* __re
   }
 }
 
-// Hadamard product, round form (FP32 working precision).  The same product as k_hadamard, scheduled
-// for targets with few interactions: a CTA owns HADR_TT targets at one frequency; the tile's pairs are
-// grouped by relative position and packed on the host into rounds of HADR_RW pairs that share one
-// position, so a warp reads each entry of that position's 8x8 block once (a shared-memory broadcast)
-// for the HADR_PPL pairs each lane holds.  Any warp may take any round; targets repeat across
-// concurrent rounds of different positions, so the accumulators are updated with shared-memory
-// atomics (the FP32 sums are therefore taken in a run-dependent order).  Two FP32 operations per
-// instruction (__ffma2_rn), with the 8x8 blocks expanded in shared memory to {re, re, -im, im}; the
-// 8 outputs of a pair are computed in HADR_NH passes to bound the registers held per lane.
-#ifndef XFMM_HADR_TT
-#define XFMM_HADR_TT 512
-#endif
-#ifndef XFMM_HADR_MINB
-#define XFMM_HADR_MINB 3
-#endif
-#ifndef XFMM_HADR_PPL
-#define XFMM_HADR_PPL 2
-#endif
-#ifndef XFMM_HADR_NH
-#define XFMM_HADR_NH 2
-#endif
-constexpr int HADR_NT = 256;                 // threads per CTA
-constexpr int HADR_TT = XFMM_HADR_TT;        // targets per tile
-constexpr int HADR_AS = HADR_TT + 1;         // accumulator row stride: [16 components][HADR_TT + 1]
-constexpr int HADR_PPL = XFMM_HADR_PPL;      // pairs per lane per round
-constexpr int HADR_RW = 32 * HADR_PPL;       // pairs per round
-constexpr int HADR_NH = XFMM_HADR_NH;        // output passes per round
-constexpr size_t hadr_smem() { return (size_t)26 * 64 * sizeof(float4) + (size_t)16 * HADR_AS * sizeof(float); }
+// Hadamard product, round form (FP32 working precision), for targets with few occupied relative
+// positions (the deepest nonleaf level).  The same product as k_hadamard, scheduled by position: a CTA
+// owns HADR_TT targets at one frequency; the tile's pairs are grouped by relative position and packed
+// on the host into rounds of HADR_RW pairs that share one position, so a warp reads each entry of that
+// position's 8x8 block once (a shared-memory broadcast) for the HADR_PPL pairs each lane holds.  Any
+// warp may take any round, and a target recurs in rounds of different positions, so each pair's 8
+// products are added to its output row with 16-byte vector atomics resolved in L2 (the sums are taken
+// in a run-dependent order); the rows are zeroed first (k_zero_rows).  Two FP32 operations per
+// instruction (__ffma2_rn), with the 8x8 blocks expanded in shared memory to {re, re, -im, im}.
+constexpr int HADR_NT = 256;            // threads per CTA
+constexpr int HADR_TT = 512;            // targets per tile
+constexpr int HADR_PPL = 2;             // pairs per lane per round
+constexpr int HADR_RW = 32 * HADR_PPL;  // pairs per round
 
-__global__ void __launch_bounds__(HADR_NT, XFMM_HADR_MINB)
+__global__ void __launch_bounds__(HADR_NT, 3)
     k_hadamard_r(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
                  const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
                  const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
-  constexpr int NW = HADR_NT / 32, TC = 8 / HADR_NH;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* sM = reinterpret_cast<float4*>(smem_raw);       // [26][64]
-  float* sAcc = reinterpret_cast<float*>(sM + 26 * 64);  // [16][HADR_AS]
+  constexpr int NW = HADR_NT / 32;
+  __shared__ float4 sM[26 * 64];
   const int tile = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
   const int lane = tid & 31, wid = tid >> 5;
   const int t0 = tile * HADR_TT;
@@ -925,14 +916,14 @@ __global__ void __launch_bounds__(HADR_NT, XFMM_HADR_MINB)
     const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + j];
     sM[e] = make_float4(m.x, m.x, -m.y, m.y);
   }
-  for (int e = tid; e < 16 * HADR_AS; e += HADR_NT) sAcc[e] = 0.f;
   __syncthreads();
   const float2* inf = in + (int64_t)f * nsrc * 8;
+  float2* of = out + (int64_t)f * ntrg * 8;
   const int r1 = tile_r[tile + 1];
   for (int r = tile_r[tile] + wid; r < r1; r += NW) {
     const float4* M = sM + rpos[r] * 64;
     int2 c[HADR_PPL];
-    float2 v[HADR_PPL][8];
+    float2 v[HADR_PPL][8], o[HADR_PPL][8];
 #pragma unroll
     for (int p = 0; p < HADR_PPL; p++) {
       c[p] = ent[(int64_t)r * HADR_RW + 32 * p + lane];
@@ -942,44 +933,41 @@ __global__ void __launch_bounds__(HADR_NT, XFMM_HADR_MINB)
 #pragma unroll
         for (int i = 0; i < 8; i++) v[p][i] = make_float2(0.f, 0.f);
       }
+#pragma unroll
+      for (int i = 0; i < 8; i++) o[p][i] = make_float2(0.f, 0.f);
     }
 #pragma unroll
-    for (int h = 0; h < HADR_NH; h++) {
-      float2 o[HADR_PPL][TC];
+    for (int sc = 0; sc < 8; sc++) {
 #pragma unroll
-      for (int p = 0; p < HADR_PPL; p++)
+      for (int i = 0; i < 8; i++) {
+        const float4 m = M[sc * 8 + i];  // {re, re, -im, im}
+        const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
 #pragma unroll
-        for (int i = 0; i < TC; i++) o[p][i] = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int sc = 0; sc < 8; sc++) {
-#pragma unroll
-        for (int i = 0; i < TC; i++) {
-          const float4 m = M[sc * 8 + h * TC + i];  // {re, re, -im, im}
-          const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
-#pragma unroll
-          for (int p = 0; p < HADR_PPL; p++) {
-            o[p][i] = __ffma2_rn(mr, v[p][sc], o[p][i]);
-            o[p][i] = __ffma2_rn(mi, make_float2(v[p][sc].y, v[p][sc].x), o[p][i]);
-          }
+        for (int p = 0; p < HADR_PPL; p++) {
+          o[p][i] = __ffma2_rn(mr, v[p][sc], o[p][i]);
+          o[p][i] = __ffma2_rn(mi, make_float2(v[p][sc].y, v[p][sc].x), o[p][i]);
         }
       }
+    }
 #pragma unroll
-      for (int p = 0; p < HADR_PPL; p++) {
-        if (c[p].x < 0) continue;
-        float* q = sAcc + c[p].y;
+    for (int p = 0; p < HADR_PPL; p++) {
+      if (c[p].x < 0) continue;
+      float4* q = reinterpret_cast<float4*>(of + (int64_t)rows[t0 + c[p].y] * 8);
 #pragma unroll
-        for (int i = 0; i < TC; i++) {
-          atomicAdd(q + (2 * (h * TC + i)) * HADR_AS, o[p][i].x);
-          atomicAdd(q + (2 * (h * TC + i) + 1) * HADR_AS, o[p][i].y);
-        }
-      }
+      for (int k = 0; k < 4; k++)
+        atomicAdd(q + k, make_float4(o[p][2 * k].x, o[p][2 * k].y, o[p][2 * k + 1].x, o[p][2 * k + 1].y));
     }
   }
-  __syncthreads();
-  float2* of = out + (int64_t)f * ntrg * 8;
-  for (int e = tid; e < HADR_TT * 8; e += HADR_NT) {
-    const int t = e >> 3, comp = 2 * (e & 7), row = rows[t0 + t];
-    if (row >= 0) of[(int64_t)row * 8 + (e & 7)] = make_float2(sAcc[comp * HADR_AS + t], sAcc[(comp + 1) * HADR_AS + t]);
+}
+
+// out[f][rows[k]][0..8) = 0 for every frequency and every listed row (-1 entries skipped)
+__global__ void k_zero_rows(float2* __restrict__ out, const int* __restrict__ rows, int nrows, int ntrg, int nfreq) {
+  const int64_t total = (int64_t)nfreq * nrows * 4;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e & 3);
+    const int64_t fr = e >> 2;
+    const int f = (int)(fr / nrows), row = rows[fr - (int64_t)f * nrows];
+    if (row >= 0) reinterpret_cast<float4*>(out + ((int64_t)f * ntrg + row) * 8)[k] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
 }
 
@@ -1733,18 +1721,17 @@ struct Engine {
       // Hadamard product
       const int ntiles = ws.had_tile0[g + 1] - ws.had_tile0[g];
       if constexpr (sizeof(CT) == 8) {
-        const size_t smem = hadr_smem();
-        if (ws.hadamard_smem < smem) {
-          XCUDA(cudaFuncSetAttribute(k_hadamard_r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-          ws.hadamard_smem = smem;
-        }
         XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
         if (ntiles > 0) {
-          k_hadamard_r<<<dim3(ntiles, nfreq), HADR_NT, smem, s>>>(
-              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
-              ws.hadr_ent.p, ws.hadr_row.p + (int64_t)ws.had_tile0[g] * HADR_TT, ns, nt, nfreq);
+          const int* rows = ws.hadr_row.p + (int64_t)ws.had_tile0[g] * HADR_TT;
+          const int nrows = ntiles * HADR_TT;
+          k_zero_rows<<<rows_grid((int64_t)nfreq * nrows * 4), 256, 0, s>>>((CT*)ws.specA.p, rows, nrows, nt, nfreq);
           XLAUNCH();
-          ws.launches++;
+          k_hadamard_r<<<dim3(ntiles, nfreq), HADR_NT, 0, s>>>(T, (const CT*)ws.specB.p, (CT*)ws.specA.p,
+                                                               ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
+                                                               ws.hadr_ent.p, rows, ns, nt, nfreq);
+          XLAUNCH();
+          ws.launches += 2;
         }
         if (ws.hadd_ld[g] > 0) {
           k_hadamard_d<<<dim3(ws.hadd_ld[g] / HADD_TT, nfreq), HADD_NT, 0, s>>>(

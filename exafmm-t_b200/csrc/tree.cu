@@ -823,6 +823,7 @@ void build_lists(Fmm& fmm, Tree& t, cudaStream_t s) {
   t.nl_level_off[t.depth + 1] = (int)nl_sorted.size();
   t.nl_by_level.upload(nl_sorted, s);
   std::vector<int> ev;
+  std::vector<int64_t> work;  // near-field pairs per evaluated leaf
   std::vector<float> sc;
   std::vector<double> sc64;
   t.p2p_pairs = t.m2p_pairs = t.l2p_pairs = 0;
@@ -835,9 +836,22 @@ void build_lists(Fmm& fmm, Tree& t, cudaStream_t s) {
       int64_t srcs = 0;
       for (int64_t j = hp_off[n]; j < hp_off[n + 1]; j++) srcs += t.h_nsrcs[hp2p[j]];
       t.p2p_pairs += srcs * t.h_ntrgs[n];
+      work.push_back(srcs * t.h_ntrgs[n]);
       t.m2p_pairs += (hm_off[n + 1] - hm_off[n]) * (int64_t)fmm.nsurf * t.h_ntrgs[n];
       t.l2p_pairs += (int64_t)fmm.nsurf * t.h_ntrgs[n];
     }
+  }
+#ifndef XFMM_SORT_EVAL
+#define XFMM_SORT_EVAL 1
+#endif
+  if (XFMM_SORT_EVAL) {
+    // evaluate the heaviest leaves first: one warp per leaf, so the grid's tail is made of small leaves
+    std::vector<int> order(ev.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+    std::vector<int> sorted(ev.size());
+    for (size_t i = 0; i < order.size(); i++) sorted[i] = ev[order[i]];
+    ev.swap(sorted);
   }
   t.n_eval_leafs = (int)ev.size();
   t.eval_leafs.upload(ev, s);
