@@ -972,94 +972,117 @@ __global__ void k_zero_rows(float2* __restrict__ out, const int* __restrict__ ro
 }
 
 // Hadamard product, dense form (FP32 working precision), for targets with most of the 26 relative
-// positions occupied.  A warp owns 64 targets (two per lane) and walks the 26 positions in order:
-// each lane multiplies its two targets' source spectra (zeros where a position is empty) by that
-// position's 8x8 block, read once per warp as a shared-memory broadcast, and keeps the sums in
-// registers, so there are no shared accumulators and no atomics; the sums are taken in a fixed order.
-// The next position's spectra are loaded while the current one is multiplied.
+// positions occupied.  A group of 4 lanes shares HADD_TPG targets; lane k of the group holds the source
+// components {2k, 2k+1}, so it loads 16 bytes of each source spectrum (a warp instruction reads whole
+// 64-byte spectra of 8 targets) and forms, for all 8 target components, the partial sums over its two
+// source components.  The group walks the 26 positions in order with the partial sums in registers;
+// each entry of a position's 8x8 block is read once per lane (rows padded so the 4 lanes of a group hit
+// distinct banks) and reused for the group's targets.  One 4-lane shuffle reduction per target at the
+// end completes the sums; no shared accumulators, no atomics, a fixed summation order.  The next
+// position's spectra are loaded while the current one is multiplied.
 #ifndef XFMM_HAD_DENSE_MIN
 #define XFMM_HAD_DENSE_MIN 12
 #endif
-constexpr int HADD_NT = 256;                 // threads per CTA
-constexpr int HADD_TT = 2 * HADD_NT;         // targets per CTA
+#ifndef XFMM_HADD_PREFETCH
+#define XFMM_HADD_PREFETCH 0  // load the next position's spectra during the current one (registers)
+#endif
+#ifndef XFMM_HADD_MINB
+#define XFMM_HADD_MINB 2
+#endif
+constexpr int HADD_NT = 256;                       // threads per CTA
+#ifndef XFMM_HADD_TPG
+#define XFMM_HADD_TPG 4
+#endif
+constexpr int HADD_TPG = XFMM_HADD_TPG;            // targets per 4-lane group
+constexpr int HADD_TT = (HADD_NT / 4) * HADD_TPG;  // targets per CTA
+constexpr int HADD_MS = 9;                         // padded row length of a block (float4 entries)
 constexpr int HAD_DENSE_MIN = XFMM_HAD_DENSE_MIN;  // occupied positions that make a target dense
-
-__device__ __forceinline__ void had_mac8x2(const float4* __restrict__ M, const float2* v0, const float2* v1,
-                                           float2* o0, float2* o1) {
-#pragma unroll
-  for (int sc = 0; sc < 8; sc++) {
-    const float2 b0 = make_float2(v0[sc].y, v0[sc].x), b1 = make_float2(v1[sc].y, v1[sc].x);
-#pragma unroll
-    for (int tc = 0; tc < 8; tc++) {
-      const float4 m = M[sc * 8 + tc];  // {re, re, -im, im}
-      const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
-      o0[tc] = __ffma2_rn(mr, v0[sc], o0[tc]);
-      o1[tc] = __ffma2_rn(mr, v1[sc], o1[tc]);
-      o0[tc] = __ffma2_rn(mi, b0, o0[tc]);
-      o1[tc] = __ffma2_rn(mi, b1, o1[tc]);
-    }
-  }
-}
-
-__device__ __forceinline__ void had_load8_or_zero(const float2* __restrict__ inf, int src, float2* v) {
-  if (src >= 0) {
-    had_load8<float2>(inf + (int64_t)src * 8, v);
-  } else {
-#pragma unroll
-    for (int i = 0; i < 8; i++) v[i] = make_float2(0.f, 0.f);
-  }
-}
 
 // tab: [26][ld] compact source index of dense target k at each position (-1: empty or padding);
 // rows: [ld] output row of dense target k (-1: padding).  ld is a multiple of HADD_TT.
-__global__ void __launch_bounds__(HADD_NT, 2)
+__global__ void __launch_bounds__(HADD_NT, XFMM_HADD_MINB)
     k_hadamard_d(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
                  const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
-  __shared__ float4 sM[26 * 64];
+  __shared__ float4 sM[26 * 8 * HADD_MS];  // [ipos][sc][tc (+pad)] = {re, re, -im, im}
   const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   for (int e = tid; e < 26 * 64; e += HADD_NT) {
-    const int j = e & 63, ipos = e >> 6;
-    const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + j];
-    sM[e] = make_float4(m.x, m.x, -m.y, m.y);
+    const int tc = e & 7, sc = (e >> 3) & 7, ipos = e >> 6;
+    const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + e - ipos * 64];
+    sM[(ipos * 8 + sc) * HADD_MS + tc] = make_float4(m.x, m.x, -m.y, m.y);
   }
   __syncthreads();
-  const int ka = blockIdx.x * HADD_TT + wid * 64 + lane, kb = ka + 32;
-  const float2* inf = in + (int64_t)f * nsrc * 8;
-  float2 oa[8], ob[8], va[8], vb[8];
+  const int g = lane >> 2, k = lane & 3;
+  // target u of this group: k0 + u*8 (the 8 groups of a warp read 8 consecutive table entries)
+  const int k0 = blockIdx.x * HADD_TT + wid * (8 * HADD_TPG) + g;
+  const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + k;  // 16 B: components 2k, 2k+1
+  float2 acc[HADD_TPG][8];
+  float4 v[HADD_TPG];
 #pragma unroll
-  for (int i = 0; i < 8; i++) oa[i] = ob[i] = make_float2(0.f, 0.f);
-  int sa = tab[ka], sb = tab[kb];
-  had_load8_or_zero(inf, sa, va);
-  had_load8_or_zero(inf, sb, vb);
+  for (int u = 0; u < HADD_TPG; u++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) acc[u][i] = make_float2(0.f, 0.f);
+    const int src = tab[k0 + u * 8];
+    v[u] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   for (int ipos = 0; ipos < 26; ipos++) {
-    int na = -1, nb = -1;
-    if (ipos + 1 < 26) {
-      na = tab[(ipos + 1) * ld + ka];
-      nb = tab[(ipos + 1) * ld + kb];
-    }
-    float2 wa[8], wb[8];
-    had_load8_or_zero(inf, na, wa);
-    had_load8_or_zero(inf, nb, wb);
-    if (__any_sync(0xffffffffu, (sa >= 0) | (sb >= 0))) had_mac8x2(sM + ipos * 64, va, vb, oa, ob);
+#if XFMM_HADD_PREFETCH
+    float4 w[HADD_TPG];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      va[i] = wa[i];
-      vb[i] = wb[i];
+    for (int u = 0; u < HADD_TPG; u++) {
+      const int src = ipos + 1 < 26 ? tab[(ipos + 1) * ld + k0 + u * 8] : -1;
+      w[u] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    sa = na;
-    sb = nb;
+#else
+    if (ipos > 0) {
+#pragma unroll
+      for (int u = 0; u < HADD_TPG; u++) {
+        const int src = tab[ipos * ld + k0 + u * 8];
+        v[u] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+#endif
+    const float4* M = sM + (ipos * 8 + 2 * k) * HADD_MS;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      float2 a[HADD_TPG], b[HADD_TPG];
+#pragma unroll
+      for (int u = 0; u < HADD_TPG; u++) {
+        a[u] = j == 0 ? make_float2(v[u].x, v[u].y) : make_float2(v[u].z, v[u].w);
+        b[u] = make_float2(a[u].y, a[u].x);
+      }
+#pragma unroll
+      for (int tc = 0; tc < 8; tc++) {
+        const float4 m = M[j * HADD_MS + tc];
+        const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
+#pragma unroll
+        for (int u = 0; u < HADD_TPG; u++) {
+          acc[u][tc] = __ffma2_rn(mr, a[u], acc[u][tc]);
+          acc[u][tc] = __ffma2_rn(mi, b[u], acc[u][tc]);
+        }
+      }
+    }
+#if XFMM_HADD_PREFETCH
+#pragma unroll
+    for (int u = 0; u < HADD_TPG; u++) v[u] = w[u];
+#endif
   }
+  // complete the sums over the 4 lanes of the group; lane k writes target components 2k, 2k+1
   float2* of = out + (int64_t)f * ntrg * 8;
-  const int ra = rows[ka], rb = rows[kb];
-  if (ra >= 0) {
-    float4* q = reinterpret_cast<float4*>(of + (int64_t)ra * 8);
 #pragma unroll
-    for (int i = 0; i < 4; i++) q[i] = make_float4(oa[2 * i].x, oa[2 * i].y, oa[2 * i + 1].x, oa[2 * i + 1].y);
-  }
-  if (rb >= 0) {
-    float4* q = reinterpret_cast<float4*>(of + (int64_t)rb * 8);
+  for (int u = 0; u < HADD_TPG; u++) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) q[i] = make_float4(ob[2 * i].x, ob[2 * i].y, ob[2 * i + 1].x, ob[2 * i + 1].y);
+    for (int tc = 0; tc < 8; tc++) {
+      acc[u][tc].x += __shfl_xor_sync(0xffffffffu, acc[u][tc].x, 1);
+      acc[u][tc].y += __shfl_xor_sync(0xffffffffu, acc[u][tc].y, 1);
+      acc[u][tc].x += __shfl_xor_sync(0xffffffffu, acc[u][tc].x, 2);
+      acc[u][tc].y += __shfl_xor_sync(0xffffffffu, acc[u][tc].y, 2);
+    }
+    const int row = rows[k0 + u * 8];
+    float4 o = make_float4(acc[u][0].x, acc[u][0].y, acc[u][1].x, acc[u][1].y);
+#pragma unroll
+    for (int kk = 1; kk < 4; kk++)
+      if (k == kk) o = make_float4(acc[u][2 * kk].x, acc[u][2 * kk].y, acc[u][2 * kk + 1].x, acc[u][2 * kk + 1].y);
+    if (row >= 0) reinterpret_cast<float4*>(of + (int64_t)row * 8)[k] = o;
   }
 }
 
