@@ -179,10 +179,47 @@ def run_ours(args, rank, world):
             e2e_step()
         torch.cuda.synchronize()
         e2e_ms = (time.perf_counter() - t0) * 1e3 / k2
-        res[prec] = dict(ms=ms, setup_s=setup_s, info=info, stages=stage_acc, clocks=clk.summary(), e2e_ms=e2e_ms)
+        fb = adjoint_timing(fmm, tree, x, q, args) if prec == "mixed" else None
+        res[prec] = dict(ms=ms, setup_s=setup_s, info=info, stages=stage_acc, clocks=clk.summary(), e2e_ms=e2e_ms,
+                         fwd_bwd=fb)
         del tree, fmm, dev_out
         torch.cuda.empty_cache()
     return res, outs, x, q
+
+
+def adjoint_timing(fmm, tree, x, q, args):
+    """Forward and forward+backward of the differentiable FMM (exafmm.autograd) on the same tree:
+    L = sum_i w_i phi_i with w ~ N(0, 1), gradients with respect to charges and coordinates."""
+    import torch
+    from exafmm.autograd import fmm_apply
+    X = torch.tensor(x, device="cuda", requires_grad=True)
+    Q = torch.tensor(q, device="cuda", requires_grad=True)
+    W = torch.tensor(np.random.default_rng(3).standard_normal(len(x)), device="cuda")
+
+    def fwd():
+        with torch.no_grad():
+            fmm_apply(Q, X, X, fmm, tree)
+
+    def fwd_bwd():
+        X.grad = Q.grad = None
+        (fmm_apply(Q, X, X, fmm, tree)[:, 0] * W).sum().backward()
+
+    times = {}
+    for name, fn in (("fwd", fwd), ("fwd_bwd", fwd_bwd)):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k = max(3, args.steps // 3)
+        e0.record()
+        for _ in range(k):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times[name] = e0.elapsed_time(e1) / k
+    return {"ms_fwd": times["fwd"], "ms_fwd_bwd": times["fwd_bwd"], "ratio": times["fwd_bwd"] / times["fwd"],
+            "note": "exafmm.autograd.fmm_apply on the bench tree (sources = targets), loss sum(w * phi), "
+                    "gradients for charges and coordinates; backward = one FMM with the cotangent as charges"}
 
 
 def accuracy(outs, x, q):
@@ -328,6 +365,7 @@ def main():
         "translations": trans,
         "stages_ms": {k: round(v, 3) for k, v in m["stages"].items() if k != "launches"},
         "setup_s": m["setup_s"],
+        "fwd_bwd": m["fwd_bwd"],
     }
     if "fp64" in res:
         f = res["fp64"]
