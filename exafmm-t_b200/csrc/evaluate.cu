@@ -1338,6 +1338,7 @@ struct Workspace {
   DBuf<char> xbuf;         // FP64: pinv input rows / output rows (contiguous, in leaf-level order)
   DBuf<char> wA, wC;       // working precision: M2M/L2L input and output rows (contiguous)
   cublasHandle_t blas = nullptr;
+  DBuf<char> blas_ws;      // the library GEMMs' workspace, fixed at creation (no allocation while capturing)
   DBuf<double> out;
   // leaves grouped by level (P2M / L2P operators are per level except for Laplace)
   std::vector<int> leaf_level_off;
@@ -1414,6 +1415,8 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   W.eq.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
   W.xbuf.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
   XCUBLAS2(cublasCreate(&W.blas));
+  W.blas_ws.alloc((size_t)32 << 20);
+  XCUBLAS2(cublasSetWorkspace(W.blas, W.blas_ws.p, W.blas_ws.bytes()));
   W.out.alloc((size_t)t.ntrg * 4 * (cplx ? 2 : 1));
   // leaf rows grouped by level: P2M (chk[pos] -> up[node]) and L2P (dn[node] -> eq[pos])
   const bool lap = f.kernel == XFMM_LAPLACE;

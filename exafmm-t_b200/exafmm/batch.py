@@ -1,0 +1,100 @@
+"""Many independent particle systems evaluated as one captured CUDA graph (no counterpart in the
+reference, which evaluates one system per call).
+
+Each system gets its own Fmm object (operators depend on the system's bounding box), tree, lists and
+device buffers for its charges and results.  One evaluate of every system (charges in, potentials
+and gradients out, all device-resident) is captured once into a CUDA graph and then replayed with a
+single launch; ``evaluate_each`` runs the same calls one system after another without the graph.
+Charges are read from ``charges[i]`` (device tensors) at every replay, so new values are picked up
+by writing into those tensors in place.  The work runs on the batch's own stream, ordered after the
+caller's current stream, which in turn waits for it: results may be read on the current stream.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _core, _lib
+
+
+class BatchedFmm:
+    """systems: list of (coords (n, 3) array, charges (n,) array); fmm_factory() -> a new Fmm object."""
+
+    def __init__(self, systems, fmm_factory, nonadaptive_depth=None):
+        self.fmms, self.trees, self.charges, self.outs = [], [], [], []
+        for coords, q in systems:
+            fmm = fmm_factory()
+            dtype = np.complex128 if fmm.kernel == "helmholtz" else np.float64
+            src = _core.init_sources(coords, np.asarray(q, dtype), fmm.kernel)
+            tree = _core.setup(src, _core.init_targets(coords), fmm, nonadaptive_depth)
+            qt = torch.tensor(np.asarray(q, dtype), device="cuda")
+            if qt.is_complex():
+                qt = torch.view_as_real(qt).reshape(-1)
+            width = 8 if fmm.kernel == "helmholtz" else 4
+            self.fmms.append(fmm)
+            self.trees.append(tree)
+            self.charges.append(qt)
+            self.outs.append(torch.zeros((len(coords), width), dtype=torch.float64, device="cuda"))
+        self.n = [len(c) for c, _ in systems]
+        self.stream = torch.cuda.Stream()
+        self.graph = None
+
+    def _enqueue(self, stream_handle):
+        L = _lib.lib()
+        st = ctypes.c_void_p(stream_handle)
+        for fmm, tree, q, out in zip(self.fmms, self.trees, self.charges, self.outs):
+            _lib.check(L.xfmm_set_charges(fmm._h, tree._h, ctypes.c_void_p(q.data_ptr()), 1, st))
+            _lib.check(L.xfmm_evaluate(fmm._h, tree._h, ctypes.c_void_p(out.data_ptr()), 1, st))
+
+    def evaluate_each(self):
+        """One evaluate per system, launched one after another on the batch stream (no graph)."""
+        self.stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(self.stream):
+            self._enqueue(self.stream.cuda_stream)
+        torch.cuda.current_stream().wait_stream(self.stream)
+        return self.outs
+
+    def capture(self):
+        """Capture one evaluate of every system into a CUDA graph.  The first evaluate of each system
+        (which sizes its work buffers) runs here, before the capture begins."""
+        self.evaluate_each()
+        self.stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=self.stream):
+            self._enqueue(self.stream.cuda_stream)
+        self.graph = g
+        return g
+
+    def replay(self):
+        """All systems in one graph launch (capture() first)."""
+        if self.graph is None:
+            raise RuntimeError("capture() before replay()")
+        self.stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(self.stream):
+            self.graph.replay()
+        torch.cuda.current_stream().wait_stream(self.stream)
+        return self.outs
+
+
+def plummer(n, rng, a=1.0, rmax=10.0):
+    """n points of a Plummer sphere with scale radius a, truncated at radius rmax."""
+    r = np.empty(0)
+    while r.size < n:
+        u = rng.random(2 * n)
+        rr = a / np.sqrt(np.maximum(u, 1e-300) ** (-2.0 / 3.0) - 1.0)
+        r = np.concatenate([r, rr[rr <= rmax]])
+    r = r[:n]
+    v = rng.standard_normal((n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True) * r[:, None]
+
+
+def batched_workload(nsys=256, nmin=2000, nmax=200000, seed=0):
+    """The batched configuration: sizes log-uniform in [nmin, nmax], half uniform-cube and half
+    Plummer systems, charges U[-1, 1)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsys)).astype(np.int64)
+    systems = []
+    for i, n in enumerate(sizes):
+        x = rng.random((n, 3)) if i % 2 == 0 else plummer(int(n), rng)
+        systems.append((x, rng.uniform(-1.0, 1.0, n)))
+    return systems
