@@ -1086,6 +1086,129 @@ __global__ void __launch_bounds__(HADD_NT, XFMM_HADD_MINB)
   }
 }
 
+// Hadamard product, dense form on the tensor cores (FP32 accuracy from three TF32 products).
+// Per frequency the dense product is a real GEMM, D[target][16] = A[target][26 x 16] B[26 x 16][16]:
+// a target's row of A holds its 26 source spectra (8 complex = 16 reals each, zero where a position is
+// empty) and B holds each position's 8x8 complex block as 2x2 real blocks ([re, im] -> [re, im]).
+// Warp-level m16n8k8 TF32 MMAs: A and B are split into TF32 heads and tails, and each position's
+// Ah Bh + Ah Bt + At Bh (small terms first; the tail-tail product, 2^-22 relative, is dropped) is
+// formed in a fresh MMA accumulator and added to FP32 running sums.  The reduction
+// index of each 8-wide step is ordered so that a lane's A fragment is one 16-byte piece of a source
+// spectrum (lane quad t of a row loads reals 4t..4t+3), and the B fragments of every (position, lane)
+// are laid out per frequency in shared memory.  A warp owns 64 targets as 4 tiles of 16 rows.
+constexpr int HADT_NT = 256;                     // threads per CTA
+constexpr int HADT_TT = (HADT_NT / 32) * 64;     // targets per CTA
+constexpr size_t HADT_SMEM = (size_t)26 * 4 * 32 * 16;
+#ifndef XFMM_HADD_TC
+#define XFMM_HADD_TC 1  // 0: dense targets on the FP32 FMA pipes (k_hadamard_d)
+#endif
+
+__device__ __forceinline__ uint32_t tf32_head(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+// head and tail of x: x = head + tail exactly, head a TF32 value
+__device__ __forceinline__ void tf32_split(float x, uint32_t& h, uint32_t& t) {
+  h = tf32_head(x);
+  t = tf32_head(x - __uint_as_float(h));
+}
+
+// tab: [26][ld] compact source index of dense target k at each position (-1: empty or padding);
+// rows: [ld] output row of dense target k (-1: padding).  ld is a multiple of HADT_TT.
+__global__ void __launch_bounds__(HADT_NT, 2)
+    k_hadamard_dt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
+                  const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
+  // sB[(ipos * 4 + c * 2 + h) * 32 + lane] = {b0 head, b1 head, b0 tail, b1 tail} of reduction step c
+  // (source components 2 t + c) and output half h (target components 4 h .. 4 h + 3) for that lane
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint4* sB = reinterpret_cast<uint4*>(smem_raw);  // 26 * 4 * 32 entries
+  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int e = tid; e < 26 * 4 * 32; e += HADT_NT) {
+    const int ln = e & 31, q = (e >> 5) & 3, ipos = e >> 7;
+    const int c = q >> 1, h = q & 1, g = ln >> 2, t = ln & 3;
+    const int sc = 2 * t + c, tc = 4 * h + (g >> 1);
+    const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + sc * 8 + tc];
+    // input real (sc, re) -> b0, (sc, im) -> b1; output real (tc, g & 1): re <- (Re m, -Im m), im <- (Im m, Re m)
+    const float v0 = (g & 1) ? m.y : m.x, v1 = (g & 1) ? m.x : -m.y;
+    uint4 b;
+    tf32_split(v0, b.x, b.z);
+    tf32_split(v1, b.y, b.w);
+    sB[e] = b;
+  }
+  __syncthreads();
+  const int g = lane >> 2, t = lane & 3;
+  const int base = blockIdx.x * HADT_TT + wid * 64 + g;  // tile j, rows g / g + 8: base + 16 j (+ 8)
+  const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + t;
+  float acc[4][2][4];
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) acc[j][h][i] = 0.f;
+  for (int ipos = 0; ipos < 26; ipos++) {
+    float4 x[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int r = 0; r < 2; r++) {
+        const int src = tab[ipos * ld + base + 16 * j + 8 * r];
+        x[j][r] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    uint4 b[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = sB[(ipos * 4 + q) * 32 + lane];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      // this position's products in a fresh MMA accumulator, then added to the running sums with
+      // round-to-nearest FP32 adds (the MMA's own accumulation is not rounded to nearest)
+      float d[2][4];
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) d[h][i] = 0.f;
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        // A fragment of step c: row g reals (4t + 2c, 4t + 2c + 1), row g + 8 the same
+        uint32_t a0h, a0t, a1h, a1t, a2h, a2t, a3h, a3t;
+        tf32_split(c == 0 ? x[j][0].x : x[j][0].z, a0h, a0t);
+        tf32_split(c == 0 ? x[j][1].x : x[j][1].z, a1h, a1t);
+        tf32_split(c == 0 ? x[j][0].y : x[j][0].w, a2h, a2t);
+        tf32_split(c == 0 ? x[j][1].y : x[j][1].w, a3h, a3t);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const uint4 bb = b[c * 2 + h];
+          mma_tf32(d[h], a0t, a1t, a2t, a3t, bb.x, bb.y);
+          mma_tf32(d[h], a0h, a1h, a2h, a3h, bb.z, bb.w);
+          mma_tf32(d[h], a0h, a1h, a2h, a3h, bb.x, bb.y);
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc[j][h][i] += d[h][i];
+    }
+  }
+  // D fragment: row g (and g + 8), columns 2t, 2t + 1 of half h = target component 4 h + t (re, im)
+  float2* of = out + (int64_t)f * ntrg * 8;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      const int row = rows[base + 16 * j + 8 * r];
+      if (row < 0) continue;
+#pragma unroll
+      for (int h = 0; h < 2; h++) of[(int64_t)row * 8 + 4 * h + t] = make_float2(acc[j][h][2 * r], acc[j][h][2 * r + 1]);
+    }
+}
+
 // ---------------------------------------------------------------- M2L transforms of the real kernels
 // The convolution grid of one child is n1^3 (n1 = 2p), index a + b n1 + c n1^2 (a fastest).  The upward
 // equivalent values occupy the corner [0, p)^3 (geometry.h:101-134, up), the downward check values are
@@ -1360,6 +1483,7 @@ struct Workspace {
   std::vector<int64_t> hadd_tab0, hadd_row0;
   std::vector<int> hadd_ld;
   size_t hadamard_smem = 0;
+  bool hadt_attr = false;
   // M2L transforms: own pruned DFT kernels (real kernels, shared memory permitting) or cuFFT on the grid
   bool fused = false;
   size_t ft_fwd_smem = 0, ft_bwd_smem = 0;
@@ -1526,7 +1650,9 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
         for (int ipos = 0; ipos < 26; ipos++) cnt += t.h_m2l_tab[26 * (size_t)tt + ipos] >= 0;
         (cnt >= HAD_DENSE_MIN ? dense : sparse).push_back(tt);
       }
-      const int ld = (int)((dense.size() + HADD_TT - 1) / HADD_TT) * HADD_TT;
+      constexpr int kAlign = HADD_TT > HADT_TT ? HADD_TT : HADT_TT;  // both dense forms tile ld exactly
+      static_assert(kAlign % HADD_TT == 0 && kAlign % HADT_TT == 0, "dense tiles must divide the table width");
+      const int ld = (int)((dense.size() + kAlign - 1) / kAlign) * kAlign;
       W.hadd_ld[g] = ld;
       W.hadd_tab0[g] = (int64_t)dtab.size();
       W.hadd_row0[g] = (int64_t)drow.size();
@@ -1760,9 +1886,19 @@ struct Engine {
           ws.launches += 2;
         }
         if (ws.hadd_ld[g] > 0) {
-          k_hadamard_d<<<dim3(ws.hadd_ld[g] / HADD_TT, nfreq), HADD_NT, 0, s>>>(
-              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
-              ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
+          if (XFMM_HADD_TC) {
+            if (!ws.hadt_attr) {
+              XCUDA(cudaFuncSetAttribute(k_hadamard_dt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
+              ws.hadt_attr = true;
+            }
+            k_hadamard_dt<<<dim3(ws.hadd_ld[g] / HADT_TT, nfreq), HADT_NT, HADT_SMEM, s>>>(
+                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+                ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
+          } else {
+            k_hadamard_d<<<dim3(ws.hadd_ld[g] / HADD_TT, nfreq), HADD_NT, 0, s>>>(
+                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+                ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
+          }
           XLAUNCH();
           ws.launches++;
         }
