@@ -1099,6 +1099,9 @@ __global__ void __launch_bounds__(HADD_NT, XFMM_HADD_MINB)
 constexpr int HADT_NT = 256;                     // threads per CTA
 constexpr int HADT_TT = (HADT_NT / 32) * 64;     // targets per CTA
 constexpr size_t HADT_SMEM = (size_t)26 * 4 * 32 * 16;
+#ifndef XFMM_HADR_TC
+#define XFMM_HADR_TC 1  // 0: sparse targets on the FP32 FMA pipes (k_hadamard_r)
+#endif
 #ifndef XFMM_HADD_TC
 #define XFMM_HADD_TC 1  // 0: dense targets on the FP32 FMA pipes (k_hadamard_d)
 #endif
@@ -1120,17 +1123,12 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t& h, uint32_t& t) {
   t = tf32_head(x - __uint_as_float(h));
 }
 
-// tab: [26][ld] compact source index of dense target k at each position (-1: empty or padding);
-// rows: [ld] output row of dense target k (-1: padding).  ld is a multiple of HADT_TT.
-__global__ void __launch_bounds__(HADT_NT, 2)
-    k_hadamard_dt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
-                  const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
-  // sB[(ipos * 4 + c * 2 + h) * 32 + lane] = {b0 head, b1 head, b0 tail, b1 tail} of reduction step c
-  // (source components 2 t + c) and output half h (target components 4 h .. 4 h + 3) for that lane
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint4* sB = reinterpret_cast<uint4*>(smem_raw);  // 26 * 4 * 32 entries
-  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  for (int e = tid; e < 26 * 4 * 32; e += HADT_NT) {
+// The B fragments of frequency f for every (position, reduction step c, output half h, lane):
+// sB[(ipos * 4 + c * 2 + h) * 32 + lane] = {b0 head, b1 head, b0 tail, b1 tail}, step c covering the
+// source components 2 t + c and half h the target components 4 h .. 4 h + 3 (t = lane % 4).
+__device__ __forceinline__ void hadt_fill_b(uint4* sB, const float2* __restrict__ T, int f, int nfreq, int tid,
+                                            int nthreads) {
+  for (int e = tid; e < 26 * 4 * 32; e += nthreads) {
     const int ln = e & 31, q = (e >> 5) & 3, ipos = e >> 7;
     const int c = q >> 1, h = q & 1, g = ln >> 2, t = ln & 3;
     const int sc = 2 * t + c, tc = 4 * h + (g >> 1);
@@ -1142,6 +1140,89 @@ __global__ void __launch_bounds__(HADT_NT, 2)
     tf32_split(v1, b.y, b.w);
     sB[e] = b;
   }
+}
+
+// D (16 x 16) += rows (x0: row g, x1: row g + 8) times the position's B, one fresh MMA accumulator:
+// d[h][0..1] = row g, target component 4 h + t (re, im); d[h][2..3] = row g + 8
+__device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, const uint4 (&b)[4], float (&d)[2][4]) {
+#pragma unroll
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) d[h][i] = 0.f;
+#pragma unroll
+  for (int c = 0; c < 2; c++) {
+    uint32_t a0h, a0t, a1h, a1t, a2h, a2t, a3h, a3t;
+    tf32_split(c == 0 ? x0.x : x0.z, a0h, a0t);
+    tf32_split(c == 0 ? x1.x : x1.z, a1h, a1t);
+    tf32_split(c == 0 ? x0.y : x0.w, a2h, a2t);
+    tf32_split(c == 0 ? x1.y : x1.w, a3h, a3t);
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const uint4 bb = b[c * 2 + h];
+      mma_tf32(d[h], a0t, a1t, a2t, a3t, bb.x, bb.y);
+      mma_tf32(d[h], a0h, a1h, a2h, a3h, bb.z, bb.w);
+      mma_tf32(d[h], a0h, a1h, a2h, a3h, bb.x, bb.y);
+    }
+  }
+}
+
+// Round form on the tensor cores: the rounds and pairs of k_hadamard_r, each round of 64 pairs as 4 row
+// tiles of 16 (pair 16 j + g and 16 j + 8 + g of tile j); lanes t and t ^ 1 trade halves so each adds
+// 16 bytes (two target components of one pair) with a vector atomic.
+__global__ void __launch_bounds__(HADR_NT, 2)
+    k_hadamard_rt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
+                  const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
+                  const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
+  constexpr int NW = HADR_NT / 32;
+  static_assert(HADR_RW == 64, "a round is 4 row tiles of 16 pairs");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint4* sB = reinterpret_cast<uint4*>(smem_raw);
+  const int tile = blockIdx.x, f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  hadt_fill_b(sB, T, f, nfreq, tid, HADR_NT);
+  __syncthreads();
+  const int t0 = tile * HADR_TT;
+  const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + t;
+  float2* of = out + (int64_t)f * ntrg * 8;
+  const int r1 = tile_r[tile + 1];
+  for (int r = tile_r[tile] + wid; r < r1; r += NW) {
+    const int ipos = rpos[r];
+    uint4 b[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = sB[(ipos * 4 + q) * 32 + lane];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int2 e0 = ent[(int64_t)r * HADR_RW + 16 * j + g], e1 = ent[(int64_t)r * HADR_RW + 16 * j + 8 + g];
+      const float4 x0 = e0.x >= 0 ? __ldg(inf + (int64_t)e0.x * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 x1 = e1.x >= 0 ? __ldg(inf + (int64_t)e1.x * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      float d[2][4];
+      hadt_tile(x0, x1, b, d);
+      const bool odd = t & 1;
+      const int2 e = odd ? e1 : e0;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        // even t keeps row g (components 4h + t, 4h + t + 1); odd t keeps row g + 8 (4h + t - 1, 4h + t)
+        const float2 send = odd ? make_float2(d[h][0], d[h][1]) : make_float2(d[h][2], d[h][3]);
+        const float rx = __shfl_xor_sync(0xffffffffu, send.x, 1), ry = __shfl_xor_sync(0xffffffffu, send.y, 1);
+        const float4 v = odd ? make_float4(rx, ry, d[h][2], d[h][3]) : make_float4(d[h][0], d[h][1], rx, ry);
+        if (e.x >= 0)
+          atomicAdd(reinterpret_cast<float4*>(of + (int64_t)rows[t0 + e.y] * 8 + 4 * h + (t & ~1)), v);
+      }
+    }
+  }
+}
+
+// tab: [26][ld] compact source index of dense target k at each position (-1: empty or padding);
+// rows: [ld] output row of dense target k (-1: padding).  ld is a multiple of HADT_TT.
+__global__ void __launch_bounds__(HADT_NT, 2)
+    k_hadamard_dt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
+                  const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
+  // sB[(ipos * 4 + c * 2 + h) * 32 + lane] = {b0 head, b1 head, b0 tail, b1 tail} of reduction step c
+  // (source components 2 t + c) and output half h (target components 4 h .. 4 h + 3) for that lane
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint4* sB = reinterpret_cast<uint4*>(smem_raw);  // 26 * 4 * 32 entries
+  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  hadt_fill_b(sB, T, f, nfreq, tid, HADT_NT);
   __syncthreads();
   const int g = lane >> 2, t = lane & 3;
   const int base = blockIdx.x * HADT_TT + wid * 64 + g;  // tile j, rows g / g + 8: base + 16 j (+ 8)
@@ -1170,26 +1251,7 @@ __global__ void __launch_bounds__(HADT_NT, 2)
       // this position's products in a fresh MMA accumulator, then added to the running sums with
       // round-to-nearest FP32 adds (the MMA's own accumulation is not rounded to nearest)
       float d[2][4];
-#pragma unroll
-      for (int h = 0; h < 2; h++)
-#pragma unroll
-        for (int i = 0; i < 4; i++) d[h][i] = 0.f;
-#pragma unroll
-      for (int c = 0; c < 2; c++) {
-        // A fragment of step c: row g reals (4t + 2c, 4t + 2c + 1), row g + 8 the same
-        uint32_t a0h, a0t, a1h, a1t, a2h, a2t, a3h, a3t;
-        tf32_split(c == 0 ? x[j][0].x : x[j][0].z, a0h, a0t);
-        tf32_split(c == 0 ? x[j][1].x : x[j][1].z, a1h, a1t);
-        tf32_split(c == 0 ? x[j][0].y : x[j][0].w, a2h, a2t);
-        tf32_split(c == 0 ? x[j][1].y : x[j][1].w, a3h, a3t);
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const uint4 bb = b[c * 2 + h];
-          mma_tf32(d[h], a0t, a1t, a2t, a3t, bb.x, bb.y);
-          mma_tf32(d[h], a0h, a1h, a2h, a3h, bb.z, bb.w);
-          mma_tf32(d[h], a0h, a1h, a2h, a3h, bb.x, bb.y);
-        }
-      }
+      hadt_tile(x[j][0], x[j][1], b, d);
 #pragma unroll
       for (int h = 0; h < 2; h++)
 #pragma unroll
@@ -1483,7 +1545,7 @@ struct Workspace {
   std::vector<int64_t> hadd_tab0, hadd_row0;
   std::vector<int> hadd_ld;
   size_t hadamard_smem = 0;
-  bool hadt_attr = false;
+  bool hadt_attr = false, hadrt_attr = false;
   // M2L transforms: own pruned DFT kernels (real kernels, shared memory permitting) or cuFFT on the grid
   bool fused = false;
   size_t ft_fwd_smem = 0, ft_bwd_smem = 0;
@@ -1879,9 +1941,19 @@ struct Engine {
           const int nrows = ntiles * HADR_TT;
           k_zero_rows<<<rows_grid((int64_t)nfreq * nrows * 4), 256, 0, s>>>((CT*)ws.specA.p, rows, nrows, nt, nfreq);
           XLAUNCH();
-          k_hadamard_r<<<dim3(ntiles, nfreq), HADR_NT, 0, s>>>(T, (const CT*)ws.specB.p, (CT*)ws.specA.p,
-                                                               ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
-                                                               ws.hadr_ent.p, rows, ns, nt, nfreq);
+          if (XFMM_HADR_TC) {
+            if (!ws.hadrt_attr) {
+              XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
+              ws.hadrt_attr = true;
+            }
+            k_hadamard_rt<<<dim3(ntiles, nfreq), HADR_NT, HADT_SMEM, s>>>(
+                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
+                ws.hadr_ent.p, rows, ns, nt, nfreq);
+          } else {
+            k_hadamard_r<<<dim3(ntiles, nfreq), HADR_NT, 0, s>>>(T, (const CT*)ws.specB.p, (CT*)ws.specA.p,
+                                                                 ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
+                                                                 ws.hadr_ent.p, rows, ns, nt, nfreq);
+          }
           XLAUNCH();
           ws.launches += 2;
         }
