@@ -30,18 +30,22 @@ def _isa():
 _LIBS = {}
 
 
-def available(nonadaptive=False):
-    name = "libxfmm_ref_%s%s.so" % ("na_" if nonadaptive else "", _isa())
-    return os.path.exists(os.path.join(REF_DIR, name))
+def _name(nonadaptive, fp32):
+    # fp32: the reference's single-precision (-DFLOAT) build, adaptive only
+    return "libxfmm_ref_%s%s.so" % ("f32_" if fp32 else ("na_" if nonadaptive else ""), _isa())
 
 
-def lib(nonadaptive=False):
-    key = bool(nonadaptive)
+def available(nonadaptive=False, fp32=False):
+    return os.path.exists(os.path.join(REF_DIR, _name(nonadaptive, fp32)))
+
+
+def lib(nonadaptive=False, fp32=False):
+    key = (bool(nonadaptive), bool(fp32))
     if key in _LIBS:
         return _LIBS[key]
     # the reference calls BLAS from inside OpenMP regions; keep OpenBLAS single-threaded
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
-    name = "libxfmm_ref_%s%s.so" % ("na_" if nonadaptive else "", _isa())
+    name = _name(nonadaptive, fp32)
     path = os.path.join(REF_DIR, name)
     if not os.path.exists(path):
         raise RuntimeError("reference oracle library missing: %s (run make -C oracle)" % path)
@@ -70,14 +74,16 @@ def _p(a):
 class RefFmm:
     """One reference FMM instance plus its tree (the state python/exafmm.cpp keeps in Tree)."""
 
-    def __init__(self, kernel, p, ncrit, wavek=0.0, nonadaptive_depth=None, datdir=None):
+    def __init__(self, kernel, p, ncrit, wavek=0.0, nonadaptive_depth=None, datdir=None, fp32=False):
         self.kernel = kernel
         self.kid = KERNELS[kernel]
         self.p, self.ncrit = p, ncrit
         self.wavek = complex(wavek)
         self.nonadaptive = nonadaptive_depth is not None
         self.depth_arg = -1 if nonadaptive_depth is None else int(nonadaptive_depth)
-        self.L = lib(self.nonadaptive)
+        if fp32 and self.nonadaptive:
+            raise ValueError("the single-precision reference build is adaptive only")
+        self.L = lib(self.nonadaptive, fp32)
         self._tmp = None
         if datdir is None:
             self._tmp = tempfile.TemporaryDirectory(prefix="xfmm_ref_")

@@ -5,7 +5,8 @@ on small seeded inputs and stores inputs, tree/list dumps and potentials+gradien
 as compressed .npz files.  Needs the reference sources (to build oracle/_ref), so
 it runs in the development container only; the fixtures it writes are committed.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py         # every fixture
+    python tests/golden/make_golden.py f32     # only the single-precision reference fixtures
 """
 import os
 import sys
@@ -40,6 +41,36 @@ CASES = [
     ("yukawa_sphere_p4", "modified_helmholtz", 10.0, 4, 32, "sphere", 2000, 0, None),
     ("helmholtz_cube_p4", "helmholtz", 5.0 + 0.0j, 4, 32, "cube", 1500, 0, None),
 ]
+
+
+# the reference's single-precision build (-DFLOAT) next to its FP64 build and FP64 direct sums at
+# every target: pins the mixed path against the reference's own FP32 FMM
+CASES_F32 = [
+    # name, kernel, wavek, p, ncrit, dist, n
+    ("f32ref_laplace_cube_p8", "laplace", 0.0, 8, 32, "cube", 8000),
+    ("f32ref_yukawa_sphere_p6", "modified_helmholtz", 10.0, 6, 32, "sphere", 5000),
+]
+
+
+def main_f32():
+    from oracle import orc
+    for i, (name, kern, k, p, ncrit, dist, n) in enumerate(CASES_F32):
+        rng = np.random.default_rng(200 + i)
+        x = points(dist, n, rng)
+        q = rng.uniform(-1, 1, n)
+        outs = {}
+        for tag, fp32 in (("out32", True), ("out64", False)):
+            f = ref.RefFmm(kern, p, ncrit, wavek=k, fp32=fp32)
+            f.setup(x, q, x)
+            outs[tag] = f.evaluate()
+            f.close()
+        # FP64 direct sums at every target (an error sampled on a subset can miss where the FP32 build
+        # is worst)
+        direct = orc.direct(kern, x, q, x, k) if kern != "laplace" else orc.direct(kern, x, q, x)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), kernel=kern, wavek=complex(k), p=p, ncrit=ncrit,
+                            src=x, q=q, direct=direct, **outs)
+        print(name, "f32 vs direct", orc.rel_l2(outs["out32"], direct), "bytes",
+              os.path.getsize(os.path.join(HERE, name + ".npz")))
 
 
 def main():
@@ -78,4 +109,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["f32"]:
+        main_f32()
+    else:
+        main()
+        main_f32()

@@ -11,7 +11,7 @@ TREE_KEYS = ["key", "ni", "nx", "leafs", "nonleafs", "src_perm", "trg_perm", "co
 
 def case_names():
     return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(f).startswith("p2p_"))
+                  if not os.path.basename(f).startswith(("p2p_", "f32ref_")))
 
 
 def load(name):
@@ -26,6 +26,16 @@ def load(name):
     d["tree"] = {k: d["tree_" + k] for k in TREE_KEYS}
     d["tree"]["depth"] = int(d["tree_depth"])
     d["tree"]["r0"] = float(d["tree_r0"])
+    return d
+
+
+def load_f32ref(name):
+    """A fixture of the reference's single-precision build (make_golden.py main_f32)."""
+    z = np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False)
+    d = {k: z[k] for k in z.files}
+    d["kernel"] = str(d["kernel"])
+    d["wavek"] = complex(d["wavek"])
+    d["p"], d["ncrit"] = int(d["p"]), int(d["ncrit"])
     return d
 
 

@@ -118,3 +118,28 @@ def test_verify_matches_oracle():
     e = fmm.verify(tree.leafs, sample=False)
     pe, ge = orc.rel_l2(out, orc.direct("laplace", g["src"], g["q"], g["trg"]))
     assert abs(e[0] - pe) < 1e-3 * pe and abs(e[1] - ge) < 1e-3 * ge
+
+
+F32_CASES = ["f32ref_laplace_cube_p8", "f32ref_yukawa_sphere_p6"]
+
+
+@pytest.mark.parametrize("name", F32_CASES)
+def test_mixed_matches_the_reference_single_precision_build(name):
+    """The mixed path against the reference's own FP32 FMM (-DFLOAT build, same inputs): at least as
+    accurate against FP64 direct sums at every target, and its output within the two errors of the
+    reference build's output."""
+    from golden_cases import load_f32ref
+    g = load_f32ref(name)
+    mod = {"laplace": "exafmm.laplace", "modified_helmholtz": "exafmm.modified_helmholtz"}[g["kernel"]]
+    import importlib
+    m = importlib.import_module(mod)
+    fmm = m.LaplaceFmm(g["p"], g["ncrit"], precision="mixed") if g["kernel"] == "laplace" else \
+        m.ModifiedHelmholtzFmm(g["p"], g["ncrit"], g["wavek"].real, precision="mixed")
+    tree = m.setup(m.init_sources(g["src"], g["q"]), m.init_targets(g["src"]), fmm)
+    out = m.evaluate(tree, fmm)
+    ex = g["direct"]  # FP64 direct sums at every target
+    ours = orc.rel_l2(out, ex)
+    theirs = orc.rel_l2(g["out32"], ex)
+    assert ours[0] <= theirs[0] and ours[1] <= theirs[1], (ours, theirs)
+    diff = orc.rel_l2(out, g["out32"])  # triangle bound: within the two errors
+    assert diff[0] <= 1.01 * (ours[0] + theirs[0]) and diff[1] <= 1.01 * (ours[1] + theirs[1]), (diff, ours, theirs)
