@@ -115,9 +115,13 @@ constexpr int EVAL_WARPS = 4;
 
 // R: arithmetic of the pair interactions; W: value type of the upward equivalent densities (M2P
 // sources).  The downward equivalent densities (L2P sources) are FP64 (the pinv output).
+#ifndef XFMM_FAR_NS32
+#define XFMM_FAR_NS32 1  // Newton steps of the FP64 far field when the working precision is FP32
+#endif
 template <int KER, class R, class W>
 __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
-  using G = Green<KER, R>;
+  // with an FP32 working precision (W), one Newton step on the FP64 reciprocal square root (~2^-44)
+  using G = Green<KER, R, std::is_same<typename Base<W>::type, float>::value ? XFMM_FAR_NS32 : 2>;
   using Q = typename G::Q;
   using A = typename Acc64<Q>::type;
   using V4 = typename R4<R>::type;
@@ -1096,8 +1100,15 @@ __global__ void __launch_bounds__(HADD_NT, XFMM_HADD_MINB)
 // index of each 8-wide step is ordered so that a lane's A fragment is one 16-byte piece of a source
 // spectrum (lane quad t of a row loads reals 4t..4t+3), and the B fragments of every (position, lane)
 // are laid out per frequency in shared memory.  A warp owns 64 targets as 4 tiles of 16 rows.
-constexpr int HADT_NT = 256;                     // threads per CTA
-constexpr int HADT_TT = (HADT_NT / 32) * 64;     // targets per CTA
+#ifndef XFMM_HADT_TILES
+#define XFMM_HADT_TILES 4  // row tiles of 16 targets per warp
+#endif
+#ifndef XFMM_HADT_PREFETCH
+#define XFMM_HADT_PREFETCH 0  // load the next position's spectra while multiplying the current ones
+#endif
+constexpr int HADT_NT = 256;                                    // threads per CTA
+constexpr int HADT_TILES = XFMM_HADT_TILES;
+constexpr int HADT_TT = (HADT_NT / 32) * 16 * HADT_TILES;      // targets per CTA
 constexpr size_t HADT_SMEM = (size_t)26 * 4 * 32 * 16;
 #ifndef XFMM_HADR_TC
 #define XFMM_HADR_TC 1  // 0: sparse targets on the FP32 FMA pipes (k_hadamard_r)
@@ -1190,15 +1201,24 @@ __global__ void __launch_bounds__(HADR_NT, 2)
     uint4 b[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) b[q] = sB[(ipos * 4 + q) * 32 + lane];
+    // the round's pairs and their spectra first (all loads in flight), then the 4 tiles
+    int2 ee[4][2];
+    float4 xx[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int rr = 0; rr < 2; rr++) ee[j][rr] = ent[(int64_t)r * HADR_RW + 16 * j + 8 * rr + g];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int rr = 0; rr < 2; rr++)
+        xx[j][rr] = ee[j][rr].x >= 0 ? __ldg(inf + (int64_t)ee[j][rr].x * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      const int2 e0 = ent[(int64_t)r * HADR_RW + 16 * j + g], e1 = ent[(int64_t)r * HADR_RW + 16 * j + 8 + g];
-      const float4 x0 = e0.x >= 0 ? __ldg(inf + (int64_t)e0.x * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 x1 = e1.x >= 0 ? __ldg(inf + (int64_t)e1.x * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
       float d[2][4];
-      hadt_tile(x0, x1, b, d);
+      hadt_tile(xx[j][0], xx[j][1], b, d);
       const bool odd = t & 1;
-      const int2 e = odd ? e1 : e0;
+      const int2 e = odd ? ee[j][1] : ee[j][0];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         // even t keeps row g (components 4h + t, 4h + t + 1); odd t keeps row g + 8 (4h + t - 1, 4h + t)
@@ -1225,29 +1245,49 @@ __global__ void __launch_bounds__(HADT_NT, 2)
   hadt_fill_b(sB, T, f, nfreq, tid, HADT_NT);
   __syncthreads();
   const int g = lane >> 2, t = lane & 3;
-  const int base = blockIdx.x * HADT_TT + wid * 64 + g;  // tile j, rows g / g + 8: base + 16 j (+ 8)
+  const int base = blockIdx.x * HADT_TT + wid * 16 * HADT_TILES + g;  // tile j, rows g / g + 8: base + 16 j (+ 8)
   const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + t;
-  float acc[4][2][4];
+  float acc[HADT_TILES][2][4];
 #pragma unroll
-  for (int j = 0; j < 4; j++)
+  for (int j = 0; j < HADT_TILES; j++)
 #pragma unroll
     for (int h = 0; h < 2; h++)
 #pragma unroll
       for (int i = 0; i < 4; i++) acc[j][h][i] = 0.f;
-  for (int ipos = 0; ipos < 26; ipos++) {
-    float4 x[4][2];
+  float4 x[HADT_TILES][2];
+#if XFMM_HADT_PREFETCH
 #pragma unroll
-    for (int j = 0; j < 4; j++)
+  for (int j = 0; j < HADT_TILES; j++)
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      const int src = tab[base + 16 * j + 8 * r];
+      x[j][r] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#endif
+  for (int ipos = 0; ipos < 26; ipos++) {
+#if XFMM_HADT_PREFETCH
+    float4 xn[HADT_TILES][2];
+#pragma unroll
+    for (int j = 0; j < HADT_TILES; j++)
+#pragma unroll
+      for (int r = 0; r < 2; r++) {
+        const int src = ipos + 1 < 26 ? tab[(ipos + 1) * ld + base + 16 * j + 8 * r] : -1;
+        xn[j][r] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#else
+#pragma unroll
+    for (int j = 0; j < HADT_TILES; j++)
 #pragma unroll
       for (int r = 0; r < 2; r++) {
         const int src = tab[ipos * ld + base + 16 * j + 8 * r];
         x[j][r] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
+#endif
     uint4 b[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) b[q] = sB[(ipos * 4 + q) * 32 + lane];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int j = 0; j < HADT_TILES; j++) {
       // this position's products in a fresh MMA accumulator, then added to the running sums with
       // round-to-nearest FP32 adds (the MMA's own accumulation is not rounded to nearest)
       float d[2][4];
@@ -1257,11 +1297,18 @@ __global__ void __launch_bounds__(HADT_NT, 2)
 #pragma unroll
         for (int i = 0; i < 4; i++) acc[j][h][i] += d[h][i];
     }
+#if XFMM_HADT_PREFETCH
+#pragma unroll
+    for (int j = 0; j < HADT_TILES; j++) {
+      x[j][0] = xn[j][0];
+      x[j][1] = xn[j][1];
+    }
+#endif
   }
   // D fragment: row g (and g + 8), columns 2t, 2t + 1 of half h = target component 4 h + t (re, im)
   float2* of = out + (int64_t)f * ntrg * 8;
 #pragma unroll
-  for (int j = 0; j < 4; j++)
+  for (int j = 0; j < HADT_TILES; j++)
 #pragma unroll
     for (int r = 0; r < 2; r++) {
       const int row = rows[base + 16 * j + 8 * r];

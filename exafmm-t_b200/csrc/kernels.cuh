@@ -50,12 +50,13 @@ __device__ __forceinline__ double2 vadd(double2 a, double2 b) { return make_doub
 // FP32: the hardware approximation.  FP64: an FP32 seed refined by two Newton-Raphson
 // steps y <- y (3 - x y^2) / 2 (quadratic convergence: ~2^-22 -> 2^-44 -> full precision),
 // the same idea as the reference's rsqrt approximation + Newton steps (vec.h:655-670).
-__device__ __forceinline__ float rsqrt_any(float x) { return rsqrtf(x); }
-__device__ __forceinline__ double rsqrt_any(double x) {
+// NS: Newton steps for FP64 (2 for FP64 results; 1, ~2^-44, where the result feeds FP32 work).
+template <int NS = 2> __device__ __forceinline__ float rsqrt_any(float x) { return rsqrtf(x); }
+template <int NS = 2> __device__ __forceinline__ double rsqrt_any(double x) {
   double y = (double)rsqrtf((float)x);
   const double hx = 0.5 * x;
-  y = y * (1.5 - hx * y * y);
-  y = y * (1.5 - hx * y * y);
+#pragma unroll
+  for (int i = 0; i < NS; i++) y = y * (1.5 - hx * y * y);
   return y;
 }
 __device__ __forceinline__ float exp_any(float x) { return __expf(x); }
@@ -68,19 +69,19 @@ __device__ __forceinline__ void sincos_any(double x, double* s, double* c) { sin
 // common 1/(4 pi) factor.  r == 0 contributes nothing (laplace.h:57, modified_helmholtz.h:61, helmholtz.h:64).
 enum KernelId { K_LAPLACE = 0, K_YUKAWA = 1, K_HELMHOLTZ = 2 };
 
-template <int KER, class R> struct Green;
+template <int KER, class R, int NS = 2> struct Green;
 
-template <class R> struct Green<K_LAPLACE, R> {
+template <class R, int NS> struct Green<K_LAPLACE, R, NS> {
   using Q = R;  // charge / value type
   R k_re, k_im;
   __device__ __forceinline__ void pot(R dx, R dy, R dz, Q q, Q& acc) const {
     const R r2 = dx * dx + dy * dy + dz * dz;
-    const R invr = r2 > R(0) ? rsqrt_any(r2) : R(0);
+    const R invr = r2 > R(0) ? rsqrt_any<NS>(r2) : R(0);
     acc += q * invr;
   }
   __device__ __forceinline__ void grad(R dx, R dy, R dz, Q q, Q& p, Q& gx, Q& gy, Q& gz) const {
     const R r2 = dx * dx + dy * dy + dz * dz;
-    const R invr = r2 > R(0) ? rsqrt_any(r2) : R(0);
+    const R invr = r2 > R(0) ? rsqrt_any<NS>(r2) : R(0);
     const R qi = q * invr;
     const R qi3 = qi * invr * invr;
     p += qi;
@@ -90,18 +91,18 @@ template <class R> struct Green<K_LAPLACE, R> {
   }
 };
 
-template <class R> struct Green<K_YUKAWA, R> {
+template <class R, int NS> struct Green<K_YUKAWA, R, NS> {
   using Q = R;
   R k_re, k_im;
   __device__ __forceinline__ void pot(R dx, R dy, R dz, Q q, Q& acc) const {
     const R r2 = dx * dx + dy * dy + dz * dz;
-    const R invr = r2 > R(0) ? rsqrt_any(r2) : R(0);
+    const R invr = r2 > R(0) ? rsqrt_any<NS>(r2) : R(0);
     const R r = r2 * invr;
     acc += q * exp_any(-k_re * r) * invr;
   }
   __device__ __forceinline__ void grad(R dx, R dy, R dz, Q q, Q& p, Q& gx, Q& gy, Q& gz) const {
     const R r2 = dx * dx + dy * dy + dz * dz;
-    const R invr = r2 > R(0) ? rsqrt_any(r2) : R(0);
+    const R invr = r2 > R(0) ? rsqrt_any<NS>(r2) : R(0);
     const R r = r2 * invr;
     const R kern = q * exp_any(-k_re * r) * invr;  // modified_helmholtz.h:159-164
     const R c = kern * (k_re * r + R(1)) * invr * invr;
@@ -112,14 +113,14 @@ template <class R> struct Green<K_YUKAWA, R> {
   }
 };
 
-template <class R> struct Green<K_HELMHOLTZ, R> {
+template <class R, int NS> struct Green<K_HELMHOLTZ, R, NS> {
   using Q = typename C2<R>::type;
   R k_re, k_im;
   // G = e^{ikr}/r = e^{-Im(k) r} (cos Re(k) r + i sin Re(k) r) / r   (helmholtz.h:241-249)
   __device__ __forceinline__ void pot(R dx, R dy, R dz, Q q, Q& acc) const {
     const R r2 = dx * dx + dy * dy + dz * dz;
     if (!(r2 > R(0))) return;
-    const R invr = rsqrt_any(r2);
+    const R invr = rsqrt_any<NS>(r2);
     const R r = r2 * invr;
     R sn, cs;
     sincos_any(k_re * r, &sn, &cs);
@@ -132,7 +133,7 @@ template <class R> struct Green<K_HELMHOLTZ, R> {
   __device__ __forceinline__ void grad(R dx, R dy, R dz, Q q, Q& p, Q& gx, Q& gy, Q& gz) const {
     const R r2 = dx * dx + dy * dy + dz * dz;
     if (!(r2 > R(0))) return;
-    const R invr = rsqrt_any(r2);
+    const R invr = rsqrt_any<NS>(r2);
     const R r = r2 * invr;
     R sn, cs;
     sincos_any(k_re * r, &sn, &cs);
