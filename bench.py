@@ -26,6 +26,11 @@ sys.path.insert(0, os.path.join(ROOT, "exafmm-t_b200"))
 
 import numpy as np  # noqa: E402
 
+try:  # the library (and the CUDA libraries it was built with) before torch; see exafmm/__init__.py
+    import exafmm  # noqa: E402,F401
+except ImportError:
+    exafmm = None
+
 METRIC = "Laplace N=4M p=8 Mparticles/s: mixed vs FP64 GPU at L2 err ≤1e-6; fwd+bwd time"
 P, NCRIT = 8, 128
 FLOPS_PER_P2P_PAIR = 28  # the reference's count for gradient P2P (laplace.h:163)

@@ -1571,6 +1571,7 @@ struct Workspace {
   DBuf<char> wA, wC;       // working precision: M2M/L2L input and output rows (contiguous)
   cublasHandle_t blas = nullptr;
   DBuf<char> blas_ws;      // the library GEMMs' workspace, fixed at creation (no allocation while capturing)
+  bool sgemm_emulated = false;  // FP32 GEMMs on the tensor cores (BF16x9 emulation)
   DBuf<double> out;
   // leaves grouped by level (P2M / L2P operators are per level except for Laplace)
   std::vector<int> leaf_level_off;
@@ -1650,6 +1651,14 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   XCUBLAS2(cublasCreate(&W.blas));
   W.blas_ws.alloc((size_t)32 << 20);
   XCUBLAS2(cublasSetWorkspace(W.blas, W.blas_ws.p, W.blas_ws.bytes()));
+#ifndef XFMM_SGEMM_BF16X9
+#define XFMM_SGEMM_BF16X9 1
+#endif
+  // FP32 translation GEMMs (M2M, L2L of the mixed path) run as the library's FP32 emulation on the
+  // tensor cores (three BF16 terms per operand, FP32 accuracy) where the loaded cuBLAS has it (12.9 and
+  // later); an older cuBLAS already loaded into the process keeps its default FP32 GEMMs
+  if (XFMM_SGEMM_BF16X9 && f.mixed())
+    W.sgemm_emulated = cublasSetMathMode(W.blas, CUBLAS_FP32_EMULATED_BF16X9_MATH) == CUBLAS_STATUS_SUCCESS;
   W.out.alloc((size_t)t.ntrg * 4 * (cplx ? 2 : 1));
   // leaf rows grouped by level: P2M (chk[pos] -> up[node]) and L2P (dn[node] -> eq[pos])
   const bool lap = f.kernel == XFMM_LAPLACE;

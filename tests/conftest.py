@@ -22,3 +22,10 @@ def golden_dir():
 PKG = os.path.join(ROOT, "exafmm-t_b200")
 if PKG not in sys.path:
     sys.path.insert(0, PKG)
+
+# load the library (and the CUDA libraries it was built with) before any test module imports torch,
+# as bench.py does; a missing build is reported by the tests themselves
+try:
+    import exafmm  # noqa: F401
+except ImportError:
+    pass
