@@ -435,7 +435,8 @@ __device__ __forceinline__ void near_leaf(const NearArgs& a, int node, int lane,
 // out structure-of-arrays so that sources (j, j+1) load as one float2, and the target's coordinates
 // are duplicated into both halves once per chunk.
 struct NearSmemF2 {
-  float hx[32], hy[32], hz[32], q[32], lx[32], ly[32], lz[32];
+  // source pair k = sources 2k, 2k+1: {hx, hy}, {hz, q}, {lx, ly}, {lz, -} as float2 pairs
+  float4 pr[16][4];
   int64_t seg_beg[NEAR_SEG];
   int seg_pre[NEAR_SEG + 1];
 };
@@ -509,16 +510,18 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
           const double4 sv = a.src4[sm.seg_beg[seg] + (pos - sm.seg_pre[seg])];
           const double dx = sv.x - c.x, dy = sv.y - c.y, dz = sv.z - c.z;
           const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
-          sm.hx[lane] = hx;
-          sm.hy[lane] = hy;
-          sm.hz[lane] = hz;
-          sm.q[lane] = (float)sv.w;
-          sm.lx[lane] = (float)(dx - (double)hx);
-          sm.ly[lane] = (float)(dy - (double)hy);
-          sm.lz[lane] = (float)(dz - (double)hz);
+          float* r = reinterpret_cast<float*>(sm.pr[lane >> 1]) + (lane & 1);  // float2 slot of this source
+          r[0] = hx;
+          r[2] = hy;
+          r[4] = hz;
+          r[6] = (float)sv.w;
+          r[8] = (float)(dx - (double)hx);
+          r[10] = (float)(dy - (double)hy);
+          r[12] = (float)(dz - (double)hz);
         } else {  // zero-charge padding far from every target
-          sm.hx[lane] = sm.hy[lane] = sm.hz[lane] = 1e3f;
-          sm.q[lane] = sm.lx[lane] = sm.ly[lane] = sm.lz[lane] = 0.f;
+          float* r = reinterpret_cast<float*>(sm.pr[lane >> 1]) + (lane & 1);
+          r[0] = r[2] = r[4] = 1e3f;
+          r[6] = r[8] = r[10] = r[12] = 0.f;
         }
         __syncwarp();
         float2 p2[TPL], gx2[TPL], gy2[TPL], gz2[TPL];
@@ -526,14 +529,12 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
         for (int u = 0; u < TPL; u++) p2[u] = gx2[u] = gy2[u] = gz2[u] = make_float2(0.f, 0.f);
 #pragma unroll 4
         for (int jj = 0; jj < npl; jj++) {
-          const int j = 2 * (jj * G2 + sub);
-          const float2 HX = *reinterpret_cast<const float2*>(&sm.hx[j]);
-          const float2 HY = *reinterpret_cast<const float2*>(&sm.hy[j]);
-          const float2 HZ = *reinterpret_cast<const float2*>(&sm.hz[j]);
-          const float2 Q = *reinterpret_cast<const float2*>(&sm.q[j]);
-          const float2 SX = *reinterpret_cast<const float2*>(&sm.lx[j]);
-          const float2 SY = *reinterpret_cast<const float2*>(&sm.ly[j]);
-          const float2 SZ = *reinterpret_cast<const float2*>(&sm.lz[j]);
+          const int jp = jj * G2 + sub;  // source pair
+          const float4 A0 = sm.pr[jp][0], A1 = sm.pr[jp][1], A2 = sm.pr[jp][2], A3 = sm.pr[jp][3];
+          const float2 HX = make_float2(A0.x, A0.y), HY = make_float2(A0.z, A0.w);
+          const float2 HZ = make_float2(A1.x, A1.y), Q = make_float2(A1.z, A1.w);
+          const float2 SX = make_float2(A2.x, A2.y), SY = make_float2(A2.z, A2.w);
+          const float2 SZ = make_float2(A3.x, A3.y);
 #pragma unroll
           for (int u = 0; u < TPL; u++) {
             // separation (t - s) from hi and lo parts
