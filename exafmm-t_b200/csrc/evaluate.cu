@@ -752,6 +752,19 @@ inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const double2* A, con
                        (const cuDoubleComplex*)A, k, &zero, (cuDoubleComplex*)C, n));
 }
 
+// Row-major C[m][n] = A[m][k] B[k][n] with leading dimensions (rows of A, B, C lda, ldb, ldc apart).
+inline void gemm_rm_ld(cublasHandle_t h, int m, int n, int k, const double* A, int lda, const double* B, int ldb,
+                       double* C, int ldc) {
+  const double one = 1.0, zero = 0.0;
+  XCUBLAS2(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, B, ldb, A, lda, &zero, C, ldc));
+}
+inline void gemm_rm_ld(cublasHandle_t h, int m, int n, int k, const double2* A, int lda, const double2* B, int ldb,
+                       double2* C, int ldc) {
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  XCUBLAS2(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, (const cuDoubleComplex*)B, ldb,
+                       (const cuDoubleComplex*)A, lda, &zero, (cuDoubleComplex*)C, ldc));
+}
+
 // ================================================================ M2L
 // grid[(s*8 + c)*nconv + g] = up[child c of source s][surface point mapped to g] (0 elsewhere)
 template <class W>
@@ -1921,8 +1934,10 @@ struct Engine {
         k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.chk.p, ws.p2m1.a.p + off, nullptr,
                                                             X + (int64_t)off * n);
         XLAUNCH();
-        gemm_rm(ws.blas, m, n, n, X + (int64_t)off * n, o.p2m1, Y + (int64_t)off * n);
-        gemm_rm(ws.blas, m, n, n, Y + (int64_t)off * n, o.p2m2, X + (int64_t)off * n);
+        // y = U^H c over the kept singular directions only (rank r <= n), then e = V S+ y
+        const int r = f.ops[KER == K_LAPLACE ? 0 : l].rank;
+        gemm_rm_ld(ws.blas, m, r, n, X + (int64_t)off * n, n, o.p2m1, n, Y + (int64_t)off * n, r);
+        gemm_rm_ld(ws.blas, m, n, r, Y + (int64_t)off * n, r, o.p2m2, n, X + (int64_t)off * n, n);
         k_rows_scatter<V64, W><<<rows_grid(tot), 256, 0, s>>>(m, n, X + (int64_t)off * n, ws.p2m2.c.p + off,
                                                              alpha_of<double>(ws.p2m2) + off, up, 0);
         XLAUNCH();
@@ -2145,8 +2160,9 @@ struct Engine {
         k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.dn.p, ws.l2p1.a.p + off,
                                                             alpha_of<double>(ws.l2p2) + off, X + (int64_t)off * n);
         XLAUNCH();
-        gemm_rm(ws.blas, m, n, n, X + (int64_t)off * n, o.l2p1, Y + (int64_t)off * n);
-        gemm_rm(ws.blas, m, n, n, Y + (int64_t)off * n, o.l2p2, X + (int64_t)off * n);
+        const int r = f.ops[KER == K_LAPLACE ? 0 : l].rank;
+        gemm_rm_ld(ws.blas, m, r, n, X + (int64_t)off * n, n, o.l2p1, n, Y + (int64_t)off * n, r);
+        gemm_rm_ld(ws.blas, m, n, r, Y + (int64_t)off * n, r, o.l2p2, n, X + (int64_t)off * n, n);
         k_rows_scatter<V64, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, X + (int64_t)off * n, ws.l2p2.c.p + off,
                                                                nullptr, (V64*)ws.eq.p, 0);
         XLAUNCH();

@@ -333,6 +333,10 @@ void precompute(Fmm& f, int depth, cudaStream_t s) {
     XREQUIRE(hinfo == 0, XFMM_ERR_NUMERIC, "check-to-equivalent SVD did not converge");
     double smax = 0;
     for (double v : hs) smax = std::max(smax, std::fabs(v));
+    // singular values come in descending order: the factors' first `rank` rows/columns carry everything
+    int rank = 0;
+    for (double v : hs) rank += v > eps * smax * 4;
+    op.rank = std::max(rank, 1);
     k_sinv<<<nb(n), 256, 0, s>>>(S.p, n, eps * smax * 4, sinv.p);
     k_svd_factors<<<nb((int64_t)n * n), 256, 0, s>>>(U.p, VT.p, sinv.p, n, cplx, F[0].p, F[1].p, F[2].p, F[3].p,
                                                       Uh.p, Vs.p);

@@ -160,6 +160,7 @@ struct LevelOps {
   DBuf<char> m2m_B;    // [8n][n]     B[c*n+k][j] = M2M[c][j][k], M2M[c] = (V S+)(U^H K_c)
   DBuf<char> l2l_B;    // [n][8n]     B[k][c*n+j] = M2M[c][k][j] (L2L = M2M^T)
   DBuf<char> m2l_T;    // [26][nfreq][64] complex: entry [s*8+t] (fmm_scale_invariant.h:549-551)
+  int rank = 0;        // singular values kept by the pinv threshold: B1 columns / B2 rows beyond are zero
 };
 
 struct Fmm {
