@@ -5,8 +5,10 @@
 //                                                        library GEMMs (pinv factors), scaled scatter (0.5^l)
 //   M2M   fmm_scale_invariant.h:233-253 / fmm.h:221-241  row gather + library GEMM per level, K = 8 nsurf
 //   P2L   fmm_base.h:127-154                             k_p2l
-//   M2L   fmm_scale_invariant.h:407-440, 560-646;        k_m2l_grid_up + cuFFT + k_transpose + k_hadamard
-//         fmm.h:395-446, 631-788                         + k_transpose + cuFFT + k_m2l_gather_dn
+//   M2L   fmm_scale_invariant.h:407-440, 560-646;        real kernels: k_m2l_fwd + k_hadamard_dt/_rt + k_m2l_bwd
+//         fmm.h:395-446, 631-788                         (FP64: k_hadamard); complex kernel or p > 10:
+//                                                        k_m2l_grid_up + cuFFT + k_transpose + Hadamard
+//                                                        + k_transpose + cuFFT + k_m2l_gather_dn
 //   L2L   fmm_scale_invariant.h:256-275 / fmm.h:244-263  row gather + library GEMM per level, N = 8 nsurf
 //   L2P   fmm_scale_invariant.h:198-230 / fmm.h:188-218  scaled row gather, two FP64 library GEMMs, scatter
 //                                                        + k_eval (far part)
@@ -811,7 +813,7 @@ void transpose(const CT* in, CT* out, int64_t R, int64_t C, cudaStream_t s) {
 // rounds of 32 lanes; rounds are built on the host so that no target occurs twice in a round, hence
 // the shared-memory accumulators need no atomics and no block barrier between positions (the sums
 // are taken in a fixed order), and each lane prefetches its next round while computing the current
-// one.  The FP32 form is k_hadamard_r below.
+// one.  The mixed path's forms run on the tensor cores (k_hadamard_dt, k_hadamard_rt below).
 constexpr int HAD_TT = 128;  // targets per CTA (4 warps x 32)
 constexpr int HAD_ST = 9;    // accumulator row stride (values): conflict-free for consecutive targets
 
@@ -831,16 +833,6 @@ template <class CT>
 __device__ __forceinline__ void had_load8(const CT* __restrict__ p, CT* v) {
 #pragma unroll
   for (int i = 0; i < 8; i++) v[i] = p[i];
-}
-template <>
-__device__ __forceinline__ void had_load8<float2>(const float2* __restrict__ p, float2* v) {
-  const float4* q = reinterpret_cast<const float4*>(p);
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const float4 w = __ldg(q + i);
-    v[2 * i] = make_float2(w.x, w.y);
-    v[2 * i + 1] = make_float2(w.z, w.w);
-  }
 }
 
 template <class CT>
@@ -906,77 +898,22 @@ __global__ void __launch_bounds__(128 * HadKC<CT>::KC) k_hadamard(const CT* __re
   }
 }
 
-// Hadamard product, round form (FP32 working precision), for targets with few occupied relative
-// positions (the deepest nonleaf level).  The same product as k_hadamard, scheduled by position: a CTA
-// owns HADR_TT targets at one frequency; the tile's pairs are grouped by relative position and packed
-// on the host into rounds of HADR_RW pairs that share one position, so a warp reads each entry of that
-// position's 8x8 block once (a shared-memory broadcast) for the HADR_PPL pairs each lane holds.  Any
-// warp may take any round, and a target recurs in rounds of different positions, so each pair's 8
-// products are added to its output row with 16-byte vector atomics resolved in L2 (the sums are taken
-// in a run-dependent order); the rows are zeroed first (k_zero_rows).  Two FP32 operations per
-// instruction (__ffma2_rn), with the 8x8 blocks expanded in shared memory to {re, re, -im, im}.
+// M2L Hadamard product of the mixed path on the tensor cores (below).  Targets are split by how many of
+// the 26 relative positions are occupied: dense targets (at least HAD_DENSE_MIN) keep their sums in
+// registers across the positions (k_hadamard_dt); sparse targets -- the deepest nonleaf level, ~7 of 26 --
+// are scheduled by position (k_hadamard_rt): a CTA owns HADR_TT sparse targets at one frequency, their
+// pairs are grouped by position and packed on the host into rounds of HADR_RW pairs that share one 8x8
+// block, and each pair's products are added to its output row with 16-byte vector atomics resolved in
+// L2 (the sums are taken in a run-dependent order) on rows zeroed first by k_zero_rows.
+// Spectra and products are frequency-major, (frequency f, node, child c) at [(f * nnodes + node) * 8 + c]:
+// a CTA (one frequency) reads its sources from one block of the spectra and writes its rows contiguously.
+#ifndef XFMM_HAD_DENSE_MIN
+#define XFMM_HAD_DENSE_MIN 12
+#endif
+constexpr int HAD_DENSE_MIN = XFMM_HAD_DENSE_MIN;  // occupied positions that make a target dense
 constexpr int HADR_NT = 256;            // threads per CTA
 constexpr int HADR_TT = 512;            // targets per tile
-constexpr int HADR_PPL = 2;             // pairs per lane per round
-constexpr int HADR_RW = 32 * HADR_PPL;  // pairs per round
-
-__global__ void __launch_bounds__(HADR_NT, 3)
-    k_hadamard_r(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
-                 const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
-                 const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
-  constexpr int NW = HADR_NT / 32;
-  __shared__ float4 sM[26 * 64];
-  const int tile = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
-  const int lane = tid & 31, wid = tid >> 5;
-  const int t0 = tile * HADR_TT;
-  for (int e = tid; e < 26 * 64; e += HADR_NT) {
-    const int j = e & 63, ipos = e >> 6;
-    const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + j];
-    sM[e] = make_float4(m.x, m.x, -m.y, m.y);
-  }
-  __syncthreads();
-  const float2* inf = in + (int64_t)f * nsrc * 8;
-  float2* of = out + (int64_t)f * ntrg * 8;
-  const int r1 = tile_r[tile + 1];
-  for (int r = tile_r[tile] + wid; r < r1; r += NW) {
-    const float4* M = sM + rpos[r] * 64;
-    int2 c[HADR_PPL];
-    float2 v[HADR_PPL][8], o[HADR_PPL][8];
-#pragma unroll
-    for (int p = 0; p < HADR_PPL; p++) {
-      c[p] = ent[(int64_t)r * HADR_RW + 32 * p + lane];
-      if (c[p].x >= 0) {
-        had_load8<float2>(inf + (int64_t)c[p].x * 8, v[p]);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 8; i++) v[p][i] = make_float2(0.f, 0.f);
-      }
-#pragma unroll
-      for (int i = 0; i < 8; i++) o[p][i] = make_float2(0.f, 0.f);
-    }
-#pragma unroll
-    for (int sc = 0; sc < 8; sc++) {
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        const float4 m = M[sc * 8 + i];  // {re, re, -im, im}
-        const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
-#pragma unroll
-        for (int p = 0; p < HADR_PPL; p++) {
-          o[p][i] = __ffma2_rn(mr, v[p][sc], o[p][i]);
-          o[p][i] = __ffma2_rn(mi, make_float2(v[p][sc].y, v[p][sc].x), o[p][i]);
-        }
-      }
-    }
-#pragma unroll
-    for (int p = 0; p < HADR_PPL; p++) {
-      if (c[p].x < 0) continue;
-      float4* q = reinterpret_cast<float4*>(of + (int64_t)rows[t0 + c[p].y] * 8);
-#pragma unroll
-      for (int k = 0; k < 4; k++)
-        atomicAdd(q + k, make_float4(o[p][2 * k].x, o[p][2 * k].y, o[p][2 * k + 1].x, o[p][2 * k + 1].y));
-    }
-  }
-}
+constexpr int HADR_RW = 64;             // pairs per round (4 row tiles of 16)
 
 // out[f][rows[k]][0..8) = 0 for every frequency and every listed row (-1 entries skipped)
 __global__ void k_zero_rows(float2* __restrict__ out, const int* __restrict__ rows, int nrows, int ntrg, int nfreq) {
@@ -986,121 +923,6 @@ __global__ void k_zero_rows(float2* __restrict__ out, const int* __restrict__ ro
     const int64_t fr = e >> 2;
     const int f = (int)(fr / nrows), row = rows[fr - (int64_t)f * nrows];
     if (row >= 0) reinterpret_cast<float4*>(out + ((int64_t)f * ntrg + row) * 8)[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-}
-
-// Hadamard product, dense form (FP32 working precision), for targets with most of the 26 relative
-// positions occupied.  A group of 4 lanes shares HADD_TPG targets; lane k of the group holds the source
-// components {2k, 2k+1}, so it loads 16 bytes of each source spectrum (a warp instruction reads whole
-// 64-byte spectra of 8 targets) and forms, for all 8 target components, the partial sums over its two
-// source components.  The group walks the 26 positions in order with the partial sums in registers;
-// each entry of a position's 8x8 block is read once per lane (rows padded so the 4 lanes of a group hit
-// distinct banks) and reused for the group's targets.  One 4-lane shuffle reduction per target at the
-// end completes the sums; no shared accumulators, no atomics, a fixed summation order.  The next
-// position's spectra are loaded while the current one is multiplied.
-#ifndef XFMM_HAD_DENSE_MIN
-#define XFMM_HAD_DENSE_MIN 12
-#endif
-#ifndef XFMM_HADD_PREFETCH
-#define XFMM_HADD_PREFETCH 0  // load the next position's spectra during the current one (registers)
-#endif
-#ifndef XFMM_HADD_MINB
-#define XFMM_HADD_MINB 2
-#endif
-constexpr int HADD_NT = 256;                       // threads per CTA
-#ifndef XFMM_HADD_TPG
-#define XFMM_HADD_TPG 4
-#endif
-constexpr int HADD_TPG = XFMM_HADD_TPG;            // targets per 4-lane group
-constexpr int HADD_TT = (HADD_NT / 4) * HADD_TPG;  // targets per CTA
-constexpr int HADD_MS = 9;                         // padded row length of a block (float4 entries)
-constexpr int HAD_DENSE_MIN = XFMM_HAD_DENSE_MIN;  // occupied positions that make a target dense
-
-// tab: [26][ld] compact source index of dense target k at each position (-1: empty or padding);
-// rows: [ld] output row of dense target k (-1: padding).  ld is a multiple of HADD_TT.
-__global__ void __launch_bounds__(HADD_NT, XFMM_HADD_MINB)
-    k_hadamard_d(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
-                 const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
-  __shared__ float4 sM[26 * 8 * HADD_MS];  // [ipos][sc][tc (+pad)] = {re, re, -im, im}
-  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  for (int e = tid; e < 26 * 64; e += HADD_NT) {
-    const int tc = e & 7, sc = (e >> 3) & 7, ipos = e >> 6;
-    const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + e - ipos * 64];
-    sM[(ipos * 8 + sc) * HADD_MS + tc] = make_float4(m.x, m.x, -m.y, m.y);
-  }
-  __syncthreads();
-  const int g = lane >> 2, k = lane & 3;
-  // target u of this group: k0 + u*8 (the 8 groups of a warp read 8 consecutive table entries)
-  const int k0 = blockIdx.x * HADD_TT + wid * (8 * HADD_TPG) + g;
-  const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + k;  // 16 B: components 2k, 2k+1
-  float2 acc[HADD_TPG][8];
-  float4 v[HADD_TPG];
-#pragma unroll
-  for (int u = 0; u < HADD_TPG; u++) {
-#pragma unroll
-    for (int i = 0; i < 8; i++) acc[u][i] = make_float2(0.f, 0.f);
-    const int src = tab[k0 + u * 8];
-    v[u] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  for (int ipos = 0; ipos < 26; ipos++) {
-#if XFMM_HADD_PREFETCH
-    float4 w[HADD_TPG];
-#pragma unroll
-    for (int u = 0; u < HADD_TPG; u++) {
-      const int src = ipos + 1 < 26 ? tab[(ipos + 1) * ld + k0 + u * 8] : -1;
-      w[u] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#else
-    if (ipos > 0) {
-#pragma unroll
-      for (int u = 0; u < HADD_TPG; u++) {
-        const int src = tab[ipos * ld + k0 + u * 8];
-        v[u] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-    }
-#endif
-    const float4* M = sM + (ipos * 8 + 2 * k) * HADD_MS;
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      float2 a[HADD_TPG], b[HADD_TPG];
-#pragma unroll
-      for (int u = 0; u < HADD_TPG; u++) {
-        a[u] = j == 0 ? make_float2(v[u].x, v[u].y) : make_float2(v[u].z, v[u].w);
-        b[u] = make_float2(a[u].y, a[u].x);
-      }
-#pragma unroll
-      for (int tc = 0; tc < 8; tc++) {
-        const float4 m = M[j * HADD_MS + tc];
-        const float2 mr = make_float2(m.x, m.y), mi = make_float2(m.z, m.w);
-#pragma unroll
-        for (int u = 0; u < HADD_TPG; u++) {
-          acc[u][tc] = __ffma2_rn(mr, a[u], acc[u][tc]);
-          acc[u][tc] = __ffma2_rn(mi, b[u], acc[u][tc]);
-        }
-      }
-    }
-#if XFMM_HADD_PREFETCH
-#pragma unroll
-    for (int u = 0; u < HADD_TPG; u++) v[u] = w[u];
-#endif
-  }
-  // complete the sums over the 4 lanes of the group; lane k writes target components 2k, 2k+1
-  float2* of = out + (int64_t)f * ntrg * 8;
-#pragma unroll
-  for (int u = 0; u < HADD_TPG; u++) {
-#pragma unroll
-    for (int tc = 0; tc < 8; tc++) {
-      acc[u][tc].x += __shfl_xor_sync(0xffffffffu, acc[u][tc].x, 1);
-      acc[u][tc].y += __shfl_xor_sync(0xffffffffu, acc[u][tc].y, 1);
-      acc[u][tc].x += __shfl_xor_sync(0xffffffffu, acc[u][tc].x, 2);
-      acc[u][tc].y += __shfl_xor_sync(0xffffffffu, acc[u][tc].y, 2);
-    }
-    const int row = rows[k0 + u * 8];
-    float4 o = make_float4(acc[u][0].x, acc[u][0].y, acc[u][1].x, acc[u][1].y);
-#pragma unroll
-    for (int kk = 1; kk < 4; kk++)
-      if (k == kk) o = make_float4(acc[u][2 * kk].x, acc[u][2 * kk].y, acc[u][2 * kk + 1].x, acc[u][2 * kk + 1].y);
-    if (row >= 0) reinterpret_cast<float4*>(of + (int64_t)row * 8)[k] = o;
   }
 }
 
@@ -1124,12 +946,6 @@ constexpr int HADT_NT = 256;                                    // threads per C
 constexpr int HADT_TILES = XFMM_HADT_TILES;
 constexpr int HADT_TT = (HADT_NT / 32) * 16 * HADT_TILES;      // targets per CTA
 constexpr size_t HADT_SMEM = (size_t)26 * 4 * 32 * 16;
-#ifndef XFMM_HADR_TC
-#define XFMM_HADR_TC 1  // 0: sparse targets on the FP32 FMA pipes (k_hadamard_r)
-#endif
-#ifndef XFMM_HADD_TC
-#define XFMM_HADD_TC 1  // 0: dense targets on the FP32 FMA pipes (k_hadamard_d)
-#endif
 
 __device__ __forceinline__ uint32_t tf32_head(float x) {
   uint32_t r;
@@ -1191,9 +1007,9 @@ __device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, co
   }
 }
 
-// Round form on the tensor cores: the rounds and pairs of k_hadamard_r, each round of 64 pairs as 4 row
-// tiles of 16 (pair 16 j + g and 16 j + 8 + g of tile j); lanes t and t ^ 1 trade halves so each adds
-// 16 bytes (two target components of one pair) with a vector atomic.
+// Round form on the tensor cores (sparse targets): each round of 64 same-position pairs as 4 row tiles of
+// 16 (pair 16 j + g and 16 j + 8 + g of tile j); lanes t and t ^ 1 trade halves so each adds 16 bytes
+// (two target components of one pair) with a vector atomic.
 __global__ void __launch_bounds__(HADR_NT, 2)
     k_hadamard_rt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
                   const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
@@ -1762,7 +1578,7 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
     W.bwd.push_back(hb);
   }
   if (f.mixed()) {
-    // Targets with at least HAD_DENSE_MIN occupied positions go to the dense form, in tiles of HADD_TT
+    // Targets with at least HAD_DENSE_MIN occupied positions go to the dense form, in tiles of HADT_TT
     // (table [26][ld], padded with -1).  The others go to the round form: tiles of HADR_TT targets;
     // per tile and relative position the pairs (source index, target index within the tile) in rounds
     // of HADR_RW, padded with source -1.  Both write disjoint rows of the group's output.
@@ -1782,9 +1598,7 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
         for (int ipos = 0; ipos < 26; ipos++) cnt += t.h_m2l_tab[26 * (size_t)tt + ipos] >= 0;
         (cnt >= HAD_DENSE_MIN ? dense : sparse).push_back(tt);
       }
-      constexpr int kAlign = HADD_TT > HADT_TT ? HADD_TT : HADT_TT;  // both dense forms tile ld exactly
-      static_assert(kAlign % HADD_TT == 0 && kAlign % HADT_TT == 0, "dense tiles must divide the table width");
-      const int ld = (int)((dense.size() + kAlign - 1) / kAlign) * kAlign;
+      const int ld = (int)((dense.size() + HADT_TT - 1) / HADT_TT) * HADT_TT;
       W.hadd_ld[g] = ld;
       W.hadd_tab0[g] = (int64_t)dtab.size();
       W.hadd_row0[g] = (int64_t)drow.size();
@@ -2013,36 +1827,24 @@ struct Engine {
           const int nrows = ntiles * HADR_TT;
           k_zero_rows<<<rows_grid((int64_t)nfreq * nrows * 4), 256, 0, s>>>((CT*)ws.specA.p, rows, nrows, nt, nfreq);
           XLAUNCH();
-          if (XFMM_HADR_TC) {
-            if (!ws.hadrt_attr) {
-              XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
-              ws.hadrt_attr = true;
-            }
-            k_hadamard_rt<<<dim3(ntiles, nfreq), HADR_NT, HADT_SMEM, s>>>(
-                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
-                ws.hadr_ent.p, rows, ns, nt, nfreq);
-          } else {
-            k_hadamard_r<<<dim3(ntiles, nfreq), HADR_NT, 0, s>>>(T, (const CT*)ws.specB.p, (CT*)ws.specA.p,
-                                                                 ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
-                                                                 ws.hadr_ent.p, rows, ns, nt, nfreq);
+          if (!ws.hadrt_attr) {
+            XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
+            ws.hadrt_attr = true;
           }
+          k_hadamard_rt<<<dim3(ntiles, nfreq), HADR_NT, HADT_SMEM, s>>>(
+              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
+              ws.hadr_ent.p, rows, ns, nt, nfreq);
           XLAUNCH();
           ws.launches += 2;
         }
         if (ws.hadd_ld[g] > 0) {
-          if (XFMM_HADD_TC) {
-            if (!ws.hadt_attr) {
-              XCUDA(cudaFuncSetAttribute(k_hadamard_dt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
-              ws.hadt_attr = true;
-            }
-            k_hadamard_dt<<<dim3(ws.hadd_ld[g] / HADT_TT, nfreq), HADT_NT, HADT_SMEM, s>>>(
-                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
-                ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
-          } else {
-            k_hadamard_d<<<dim3(ws.hadd_ld[g] / HADD_TT, nfreq), HADD_NT, 0, s>>>(
-                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
-                ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
+          if (!ws.hadt_attr) {
+            XCUDA(cudaFuncSetAttribute(k_hadamard_dt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
+            ws.hadt_attr = true;
           }
+          k_hadamard_dt<<<dim3(ws.hadd_ld[g] / HADT_TT, nfreq), HADT_NT, HADT_SMEM, s>>>(
+              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+              ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
           XLAUNCH();
           ws.launches++;
         }
