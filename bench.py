@@ -285,17 +285,19 @@ def roofline(r, peaks, src):
                  + nt * spec + nt * 8 * nsurf * 4 * 2)  # backward: products in, dn read-modify-write
     m2l_ms = st["M2L_fft"] + st["M2L_hadamard"] + st["M2L_ifft"]
     m2l = {"bound": "hbm", "achieved": m2l_bytes / (m2l_ms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-           "kernel": "k_m2l_fwd + k_hadamard_d/k_hadamard_r + k_m2l_bwd (M2L)", "algorithmic_bytes": m2l_bytes,
+           "kernel": "k_m2l_fwd + k_hadamard_dt/k_hadamard_rt (tensor cores) + k_m2l_bwd (M2L)", "algorithmic_bytes": m2l_bytes,
            "ms": m2l_ms, "ms_transforms": st["M2L_fft"] + st["M2L_ifft"], "ms_hadamard": st["M2L_hadamard"],
            "peak_source": src}
     m2l["frac"] = m2l["achieved"] / m2l["peak"]
     nl = info["nleafs"]
-    pinv_flops = 4 * 2.0 * nl * nsurf * nsurf  # two FP64 GEMMs each for P2M and L2P
+    rank = {6: 152, 8: 255, 10: 319}.get(P, nsurf)  # singular values the 4e-10 threshold keeps (Laplace)
+    pinv_flops = 4 * 2.0 * nl * nsurf * rank  # two FP64 GEMMs each for P2M and L2P, truncated to the rank
     tr_flops = 2 * 2.0 * (info["nnonleafs"]) * nsurf * 8 * nsurf  # M2M + L2L
     trans = {"pinv_fp64_tflops": pinv_flops / ((st["P2M"] + st["L2P_dc2e"]) * 1e-3) / 1e12,
              "m2m_l2l_fp32_tflops": tr_flops / ((st["M2M"] + st["L2L"]) * 1e-3) / 1e12,
-             "note": "library GEMMs (FP64 and FP32, not tensor-core TF32: the FP32 translations keep the 1e-6 error "
-                     "budget); stage times include the row gather/scatter kernels and, for P2M, the check potentials"}
+             "note": "library GEMMs: FP64 pinv factors on the FP64 tensor cores, truncated to the kept singular "
+                     "values; FP32 M2M/L2L as cuBLAS BF16x9 emulation on the tensor cores (FP32 accuracy); stage "
+                     "times include the row gather/scatter kernels and, for P2M, the check potentials"}
     return near, m2l, trans
 
 
