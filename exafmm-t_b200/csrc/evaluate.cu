@@ -143,8 +143,10 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
   using Q64 = typename Acc64<Q>::type;
   const W* upv = (const W*)a.up;
   const Q64* eqv = (const Q64*)a.eq;
-  for (int t0 = 0; t0 < T; t0 += 32) {
-    const int Tc = min(32, T - t0);
+  for (int t0 = 0, Tc = 0; t0 < T; t0 += Tc) {
+    // blocks of 32 targets, the last 17..32 as 16 + the rest, so that the split of the sources over
+    // 2..32 lanes per target keeps the lanes busy
+    Tc = T - t0 > 32 ? 32 : (T - t0 > 16 ? 16 : T - t0);
     int G2 = 1;  // lanes per target: source stride
     while (G2 * 2 * Tc <= 32) G2 *= 2;
     const int tl = lane / G2, sub = lane % G2;
