@@ -20,10 +20,12 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <type_traits>
 #include <cmath>
 
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 #include "xfmm_internal.h"
 
 namespace xfmm {
@@ -278,6 +280,10 @@ struct NearArgs {
   const double* src_qim;
   double* out;
   double k_re, k_im;
+  // Laplace paired-FP32 form: sources split once per evaluate into FP32 hi/lo parts relative to
+  // (ox, oy, oz), two float4 per source: {hx, hy, hz, q}, {lx, ly, lz, 0}
+  const float4* srcf;
+  double ox, oy, oz;
 };
 
 template <class R> struct Stage4;
@@ -438,9 +444,19 @@ __device__ __forceinline__ void near_leaf(const NearArgs& a, int node, int lane,
 // sm_100 paired FP32 operations (__ffma2_rn / __fadd2_rn / __fmul2_rn): the staged sources are laid
 // out structure-of-arrays so that sources (j, j+1) load as one float2, and the target's coordinates
 // are duplicated into both halves once per chunk.
+// Coordinates are split into FP32 hi + lo parts relative to one origin (the root centre) for the
+// whole evaluate: the separation (th - sh) + (tl - sl) is then accurate to a few FP32 ulps of itself
+// however close the pair is (the hi difference is rounded once, relative to its own size, and the lo
+// parts carry the residuals of both coordinates), so the sources are split once per evaluate
+// (k_src_split) instead of once per target leaf that stages them.
+#ifndef XFMM_NEAR_CH
+#define XFMM_NEAR_CH 64
+#endif
+constexpr int NEAR_CH = XFMM_NEAR_CH;  // sources staged per chunk (32 or 64)
+static_assert(NEAR_CH == 32 || NEAR_CH == 64, "NEAR_CH");
 struct NearSmemF2 {
   // source pair k = sources 2k, 2k+1: {hx, hy}, {hz, q}, {lx, ly}, {lz, -} as float2 pairs
-  float4 pr[16][4];
+  float4 pr[NEAR_CH / 2][4];
   int64_t seg_beg[NEAR_SEG];
   int seg_pre[NEAR_SEG + 1];
 };
@@ -451,13 +467,12 @@ template <int TPL>
 __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, int lane, NearSmemF2& sm) {
   const int T = a.ntrgs[node];
   const int64_t tb = a.tbeg[node];
-  const double4 c = a.center[node];
   const int64_t e0 = a.p2p_off[node], e1 = a.p2p_off[node + 1];
-  int G2 = 1;  // at most 16 lanes per target: each lane takes at least one source pair per chunk
+  int G2 = 1;  // at most 16 lanes per target
   if (TPL == 1)
     while (G2 * 2 * T <= 32 && G2 < 16) G2 *= 2;
   const int tl = lane / G2, sub = lane % G2;
-  const int npl = 16 / G2;  // source pairs per lane per chunk
+  const int npl = NEAR_CH / 2 / G2;  // source pairs per lane per chunk
   const float2 M1 = make_float2(-1.f, -1.f);
   for (int t0 = 0; t0 < T; t0 += 32 * TPL) {
     float2 TX[TPL], TY[TPL], TZ[TPL], LX[TPL], LY[TPL], LZ[TPL];
@@ -468,9 +483,9 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
       double dx = 0, dy = 0, dz = 0;
       if (t < T) {
         const double4 v = a.trg4[tb + t];
-        dx = v.x - c.x;
-        dy = v.y - c.y;
-        dz = v.z - c.z;
+        dx = v.x - a.ox;
+        dy = v.y - a.oy;
+        dz = v.z - a.oz;
       }
       const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
       TX[u] = dup2(hx);
@@ -506,26 +521,27 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
       __syncwarp();
       const int total = carry;
       int seg = 0;
-      for (int p0 = 0; p0 < total; p0 += 32) {
-        const int pos = p0 + lane;
+      for (int p0 = 0; p0 < total; p0 += NEAR_CH) {
         __syncwarp();
-        if (pos < total) {
-          while (sm.seg_pre[seg + 1] <= pos) seg++;
-          const double4 sv = a.src4[sm.seg_beg[seg] + (pos - sm.seg_pre[seg])];
-          const double dx = sv.x - c.x, dy = sv.y - c.y, dz = sv.z - c.z;
-          const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
-          float* r = reinterpret_cast<float*>(sm.pr[lane >> 1]) + (lane & 1);  // float2 slot of this source
-          r[0] = hx;
-          r[2] = hy;
-          r[4] = hz;
-          r[6] = (float)sv.w;
-          r[8] = (float)(dx - (double)hx);
-          r[10] = (float)(dy - (double)hy);
-          r[12] = (float)(dz - (double)hz);
-        } else {  // zero-charge padding far from every target
-          float* r = reinterpret_cast<float*>(sm.pr[lane >> 1]) + (lane & 1);
-          r[0] = r[2] = r[4] = 1e3f;
-          r[6] = r[8] = r[10] = r[12] = 0.f;
+#pragma unroll
+        for (int h = 0; h < NEAR_CH / 32; h++) {
+          const int pos = p0 + 32 * h + lane;
+          // zero-charge padding: contributes 0 wherever it lies (r == 0 is masked below)
+          float4 hi = make_float4(0.f, 0.f, 0.f, 0.f), lo = hi;
+          if (pos < total) {
+            while (sm.seg_pre[seg + 1] <= pos) seg++;
+            const int64_t si = sm.seg_beg[seg] + (pos - sm.seg_pre[seg]);
+            hi = a.srcf[2 * si];
+            lo = a.srcf[2 * si + 1];
+          }
+          float* r = reinterpret_cast<float*>(sm.pr[16 * h + (lane >> 1)]) + (lane & 1);  // float2 slot
+          r[0] = hi.x;
+          r[2] = hi.y;
+          r[4] = hi.z;
+          r[6] = hi.w;
+          r[8] = lo.x;
+          r[10] = lo.y;
+          r[12] = lo.z;
         }
         __syncwarp();
         float2 p2[TPL], gx2[TPL], gy2[TPL], gz2[TPL];
@@ -949,11 +965,11 @@ constexpr int HADT_TILES = XFMM_HADT_TILES;
 constexpr int HADT_TT = (HADT_NT / 32) * 16 * HADT_TILES;      // targets per CTA
 constexpr size_t HADT_SMEM = (size_t)26 * 4 * 32 * 16;
 
-__device__ __forceinline__ uint32_t tf32_head(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
+// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away from zero: half of the 13
+// dropped bits' range is added to the magnitude and the dropped bits are cleared (a carry moves into
+// the exponent when the rounding crosses a binade).  Integer ALU work, where the conversion instruction
+// would run on the much narrower transcendental/conversion pipe.
+__device__ __forceinline__ uint32_t tf32_head(float x) { return (__float_as_uint(x) + 0x1000u) & 0xffffe000u; }
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
                                          uint32_t b1) {
   asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
@@ -964,6 +980,13 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
 __device__ __forceinline__ void tf32_split(float x, uint32_t& h, uint32_t& t) {
   h = tf32_head(x);
   t = tf32_head(x - __uint_as_float(h));
+}
+// The same split with the tail left unrounded, for operands split on every use: the tensor core reads
+// only a TF32 operand's top 19 bits, so the tail (at most 12 significant bits after a round-to-nearest
+// head) is truncated there instead, an error below 2^-22 |x| of either sign.
+__device__ __forceinline__ void tf32_split_a(float x, uint32_t& h, uint32_t& t) {
+  h = tf32_head(x);
+  t = __float_as_uint(x - __uint_as_float(h));
 }
 
 // The B fragments of frequency f for every (position, reduction step c, output half h, lane):
@@ -995,10 +1018,10 @@ __device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, co
 #pragma unroll
   for (int c = 0; c < 2; c++) {
     uint32_t a0h, a0t, a1h, a1t, a2h, a2t, a3h, a3t;
-    tf32_split(c == 0 ? x0.x : x0.z, a0h, a0t);
-    tf32_split(c == 0 ? x1.x : x1.z, a1h, a1t);
-    tf32_split(c == 0 ? x0.y : x0.w, a2h, a2t);
-    tf32_split(c == 0 ? x1.y : x1.w, a3h, a3t);
+    tf32_split_a(c == 0 ? x0.x : x0.z, a0h, a0t);
+    tf32_split_a(c == 0 ? x1.x : x1.z, a1h, a1t);
+    tf32_split_a(c == 0 ? x0.y : x0.w, a2h, a2t);
+    tf32_split_a(c == 0 ? x1.y : x1.w, a3h, a3t);
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       const uint4 bb = b[c * 2 + h];
@@ -1148,6 +1171,200 @@ __global__ void __launch_bounds__(HADT_NT, 2)
 #pragma unroll
       for (int h = 0; h < 2; h++) of[(int64_t)row * 8 + 4 * h + t] = make_float2(acc[j][h][2 * r], acc[j][h][2 * r + 1]);
     }
+}
+
+// Hadamard product, dense form on the sm_100 tensor cores through tcgen05 (FP32 accuracy from three TF32
+// products, as in k_hadamard_dt).  A CTA of 128 threads owns 128 dense targets -- thread i, target slot i
+// of the tile, TMEM lane i -- and HADC_FPB frequencies.  Per frequency the 26 positions' B blocks
+// (16 x 16 reals, TF32 head and tail) are laid out in shared memory as K-major core matrices.  Per
+// position every thread gathers its target's source spectrum (16 reals), splits it into TF32 head and
+// tail and stores both into TMEM (operand A); one thread then issues the position's six M128 N16 K8 MMAs
+// (A tail x B head, A head x B tail, A head x B head per 8-wide step) into a fresh TMEM accumulator and
+// commits them to an mbarrier.  A and D are double-buffered: the MMAs of one position run while the
+// threads gather and split the next, and each position's products are read back (tcgen05.ld) two
+// positions later and added to FP32 running sums in registers with round-to-nearest adds (the tensor
+// core's own accumulation is not rounded to nearest, so it never spans more than one position).
+// Every wait is bounded; a wait that runs out ends the CTA's work and sets *status.
+constexpr int HADC_NT = 128;
+#ifndef XFMM_HADC_FPB
+#define XFMM_HADC_FPB 2
+#endif
+constexpr int HADC_FPB = XFMM_HADC_FPB;                   // frequencies per CTA
+constexpr size_t HADC_SMEM = (size_t)26 * 2 * 1024;        // B of one frequency: [position][head, tail], 1 KB each
+constexpr uint32_t HADC_TMEM_COLS = 128;                   // A: 2 x (16 head + 16 tail) columns, D: 2 x 16 columns
+constexpr uint32_t HADC_D = 64;                            // first D column
+constexpr long long HADC_WAIT = 2000000000LL;              // SM cycles (about a second) before a wait gives up
+
+// The A columns (reduction index) are a permutation of the 16 input reals fixed by the TMEM store shape
+// (16x256b): the 4 lanes of a quad load one source spectrum as 4 contiguous 16-byte pieces, lane q the
+// reals 4q .. 4q + 3, which land in columns 2q, 2q + 1, 8 + 2q, 9 + 2q.  Column of input real k:
+__device__ __forceinline__ int hadc_col(int k) {
+  const int q = k >> 2, r = k & 3;
+  return r < 2 ? 2 * q + r : 8 + 2 * q + (r - 2);
+}
+// byte offset of B element (output real n, A column c) in the 1 KB block of one (position, part):
+// core matrix (c / 4, n / 8) at 256 (c / 4) + 128 (n / 8), its row n % 8 at 16 (n % 8), column c % 4
+__device__ __forceinline__ uint32_t hadc_boff(int n, int c) {
+  return (uint32_t)((c >> 2) * 256 + (n >> 3) * 128 + (n & 7) * 16 + (c & 3) * 4);
+}
+// lane (g, q)'s pieces of the spectra of its warp's rows g, g + 8, g + 16, g + 24 (one index per lane in idx)
+__device__ __forceinline__ void hadc_load(float4 (&x)[4], const float4* __restrict__ inf, int idx, int g, int q) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int src = __shfl_sync(0xffffffffu, idx, g + 8 * i);
+    x[i] = src >= 0 ? __ldg(inf + (int64_t)src * 4 + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+__global__ void __launch_bounds__(HADC_NT, 4)
+    k_hadamard_dc(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
+                  const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq,
+                  int* __restrict__ status) {
+  using namespace tc5;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
+  const int k = blockIdx.x * HADC_NT + tid;  // dense target slot (TMEM lane tid)
+  const uint32_t sB = smem_u32(smem_raw);
+  const uint32_t bar0 = smem_u32(&mbar[0]);  // barrier of buffer s at bar0 + 8 s
+  if (wid == 0) {
+    tmem_alloc(smem_u32(&tmem_base), HADC_TMEM_COLS);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(bar0, 1);
+    mbar_init(bar0 + 8, 1);
+    fence_mbar_init();
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tm = __shfl_sync(0xffffffffu, tmem_base, 0);  // warp-uniform
+  const uint32_t tw = tm + ((uint32_t)(wid * 32) << 16);          // this warp's quarter of the lanes
+  constexpr uint32_t IDESC = idesc_tf32(128, 16);
+  const int row = rows[k];
+  uint32_t ph = 0;    // bit s: parity of the next phase of buffer s's barrier to wait for
+  uint32_t pend = 0;  // bit s: MMAs committed to buffer s's barrier and not yet waited for
+  bool ok = true;
+  for (int fi = 0; fi < HADC_FPB && ok; fi++) {
+    const int f = blockIdx.y * HADC_FPB + fi;
+    if (f >= nfreq) break;
+    // B of frequency f: factor m(sc, tc) of position ipos -> the real 2 x 2 block (outputs 2 tc, 2 tc + 1;
+    // inputs 2 sc, 2 sc + 1) = [[Re m, -Im m], [Im m, Re m]], split into TF32 head (first KB) and tail
+    for (int e = tid; e < 26 * 64; e += HADC_NT) {
+      const int ipos = e >> 6, sc = (e >> 3) & 7, tc = e & 7;
+      const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + sc * 8 + tc];
+      const float v[4] = {m.x, -m.y, m.y, m.x};
+      unsigned char* blk = smem_raw + ipos * 2048;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint32_t off = hadc_boff(2 * tc + (j >> 1), hadc_col(2 * sc + (j & 1)));
+        uint32_t h, t;
+        tf32_split(v[j], h, t);
+        *reinterpret_cast<uint32_t*>(blk + off) = h;
+        *reinterpret_cast<uint32_t*>(blk + 1024 + off) = t;
+      }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8);
+    float acc[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) acc[i] = 0.f;
+    float4 x[4];
+    hadc_load(x, inf, tab[k], g, q);
+    int srcn = tab[ld + k];  // this lane's row, next position
+#pragma unroll 2
+    for (int p = 0; p < 26; p++) {
+      const int s = p & 1;
+      float4 xn[4];
+      if (p + 1 < 26) hadc_load(xn, inf, srcn, g, q);
+      if (p + 2 < 26) srcn = tab[(p + 2) * ld + k];
+      if (pend >> s & 1) {  // products of position p - 2
+        ok = mbar_wait(bar0 + 8 * s, ph >> s & 1, HADC_WAIT);
+        ph ^= 1u << s;
+        pend &= ~(1u << s);
+        if (ok) {
+          fence_after_sync();
+          uint32_t d[16];
+          ld_32x32b_x16(tw + HADC_D + 16 * s, d);
+          wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; i++) acc[i] += __uint_as_float(d[i]);
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {  // rows 16 h + g (x[2h]) and 16 h + g + 8 (x[2h + 1]) of the warp
+        const float4 a = x[2 * h], b = x[2 * h + 1];
+        const float xs[8] = {a.x, a.y, b.x, b.y, a.z, a.w, b.z, b.w};
+        uint32_t ah[8], at[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) tf32_split_a(xs[i], ah[i], at[i]);
+        const uint32_t ta = tw + ((uint32_t)(16 * h) << 16) + 32 * s;
+        st_16x256b_x2(ta, ah);
+        st_16x256b_x2(ta + 16, at);
+      }
+      wait_st();
+      fence_before_sync();
+      if (!__syncthreads_and(ok)) {
+        ok = false;
+        break;
+      }
+      if (wid == 0) {
+        fence_after_sync();
+        if (elect_one()) {
+          const uint32_t dd = tm + HADC_D + 16 * s, aa = tm + 32 * s, bb = sB + p * 2048;
+#pragma unroll
+          for (int kk = 0; kk < 2; kk++) {
+            const uint64_t bh = sdesc_nosw(bb + 512 * kk, 256, 128), bt = sdesc_nosw(bb + 1024 + 512 * kk, 256, 128);
+            mma_tf32_ts(dd, aa + 16 + 8 * kk, bh, IDESC, kk);  // fresh sums at the first step
+            mma_tf32_ts(dd, aa + 8 * kk, bt, IDESC, 1);
+            mma_tf32_ts(dd, aa + 8 * kk, bh, IDESC, 1);
+          }
+          commit(bar0 + 8 * s);
+        }
+        __syncwarp();
+      }
+      pend |= 1u << s;
+#pragma unroll
+      for (int i = 0; i < 4; i++) x[i] = xn[i];
+    }
+    // the last two positions' products
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      if (!ok || !(pend >> s & 1)) continue;
+      ok = mbar_wait(bar0 + 8 * s, ph >> s & 1, HADC_WAIT);
+      ph ^= 1u << s;
+      pend &= ~(1u << s);
+      if (ok) {
+        fence_after_sync();
+        uint32_t d[16];
+        ld_32x32b_x16(tw + HADC_D + 16 * s, d);
+        wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; i++) acc[i] += __uint_as_float(d[i]);
+      }
+    }
+    if (ok && row >= 0) {
+      float4* o = reinterpret_cast<float4*>(out + ((int64_t)f * ntrg + row) * 8);
+#pragma unroll
+      for (int i = 0; i < 4; i++) o[i] = make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);
+    }
+    fence_before_sync();
+    ok = __syncthreads_and(ok);  // every thread done with this frequency's B and D before the next fill
+    fence_after_sync();
+  }
+  // on an early end, give the MMAs still in flight a bounded time to finish before the TMEM is released
+  for (int s = 0; s < 2; s++)
+    if (pend >> s & 1) mbar_wait(bar0 + 8 * s, ph >> s & 1, HADC_WAIT);
+  fence_before_sync();
+  __syncthreads();
+  if (wid == 0) {
+    fence_after_sync();
+    tmem_dealloc(tm, HADC_TMEM_COLS);
+  }
+  if (!ok && tid == 0) atomicExch(status, 1);
 }
 
 // ---------------------------------------------------------------- M2L transforms of the real kernels
@@ -1365,6 +1582,17 @@ __global__ void k_m2l_gather_dn(const int* __restrict__ trg, int ntrg, const int
 }
 
 // ================================================================ misc
+// Sources of the Laplace paired-FP32 near field: hi/lo FP32 parts of (x - o), FP32 charge.
+__global__ void k_src_split(const double4* __restrict__ src4, int64_t n, double ox, double oy, double oz,
+                            float4* __restrict__ srcf) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 v = src4[i];
+  const double dx = v.x - ox, dy = v.y - oy, dz = v.z - oz;
+  const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
+  srcf[2 * i] = make_float4(hx, hy, hz, (float)v.w);
+  srcf[2 * i + 1] = make_float4((float)(dx - (double)hx), (float)(dy - (double)hy), (float)(dz - (double)hz), 0.f);
+}
 __global__ void k_set_charges(const double* __restrict__ q, const int* __restrict__ perm, int64_t n, int cplx,
                               double4* __restrict__ src4, double* __restrict__ qim) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1405,6 +1633,8 @@ struct Workspace {
   DBuf<char> blas_ws;      // the library GEMMs' workspace, fixed at creation (no allocation while capturing)
   bool sgemm_emulated = false;  // FP32 GEMMs on the tensor cores (BF16x9 emulation)
   DBuf<double> out;
+  DBuf<float4> srcf;  // Laplace mixed near field: per source {hx, hy, hz, q}, {lx, ly, lz, 0}
+  DBuf<int> status;   // set by a kernel whose bounded wait ran out (0: none)
   // leaves grouped by level (P2M / L2P operators are per level except for Laplace)
   std::vector<int> leaf_level_off;
   GemmRows p2m1, p2m2, l2p1, l2p2;  // two factors each (rows grouped by leaf level)
@@ -1425,7 +1655,10 @@ struct Workspace {
   std::vector<int64_t> hadd_tab0, hadd_row0;
   std::vector<int> hadd_ld;
   size_t hadamard_smem = 0;
-  bool hadt_attr = false, hadrt_attr = false;
+  bool hadt_attr = false, hadrt_attr = false, hadc_attr = false;
+  // dense Hadamard targets on tcgen05 (k_hadamard_dc) instead of mma.sync (k_hadamard_dt): chosen when the
+  // workspace is created, by XFMM_HADAMARD_TCGEN05=1 in the environment
+  bool had_tc5 = false;
   // M2L transforms: own pruned DFT kernels (real kernels, shared memory permitting) or cuFFT on the grid
   bool fused = false;
   size_t ft_fwd_smem = 0, ft_bwd_smem = 0;
@@ -1492,6 +1725,13 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   if (XFMM_SGEMM_BF16X9 && f.mixed())
     W.sgemm_emulated = cublasSetMathMode(W.blas, CUBLAS_FP32_EMULATED_BF16X9_MATH) == CUBLAS_STATUS_SUCCESS;
   W.out.alloc((size_t)t.ntrg * 4 * (cplx ? 2 : 1));
+  W.status.alloc(1);
+  {
+    const char* e = std::getenv("XFMM_HADAMARD_TCGEN05");
+    W.had_tc5 = e && e[0] == '1';
+  }
+  XCUDA(cudaMemsetAsync(W.status.p, 0, sizeof(int), s));
+  if (f.kernel == XFMM_LAPLACE && f.mixed()) W.srcf.alloc(2 * (size_t)std::max<int64_t>(t.nsrc, 1));
   // leaf rows grouped by level: P2M (chk[pos] -> up[node]) and L2P (dn[node] -> eq[pos])
   const bool lap = f.kernel == XFMM_LAPLACE;
   std::vector<int> order(t.nleafs);
@@ -1839,7 +2079,17 @@ struct Engine {
           XLAUNCH();
           ws.launches += 2;
         }
-        if (ws.hadd_ld[g] > 0) {
+        if (ws.hadd_ld[g] > 0 && ws.had_tc5) {
+          if (!ws.hadc_attr) {
+            XCUDA(cudaFuncSetAttribute(k_hadamard_dc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADC_SMEM));
+            ws.hadc_attr = true;
+          }
+          k_hadamard_dc<<<dim3(ws.hadd_ld[g] / HADC_NT, (nfreq + HADC_FPB - 1) / HADC_FPB), HADC_NT, HADC_SMEM, s>>>(
+              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+              ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq, ws.status.p);
+          XLAUNCH();
+          ws.launches++;
+        } else if (ws.hadd_ld[g] > 0) {
           if (!ws.hadt_attr) {
             XCUDA(cudaFuncSetAttribute(k_hadamard_dt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
             ws.hadt_attr = true;
@@ -1982,11 +2232,17 @@ struct Engine {
                  t.p2p.p,        t.m2p.p,   f.surf_base.p, n,        ws.up.p,       ws.eq.p,        ws.out.p,
                  f.k_re,         f.k_im,    1,           1,         0,             1};
       const int blocks = nblk(t.n_eval_leafs, EVAL_WARPS);
-      NearArgs na{t.eval_leafs.p, t.leafs.p, t.nsrcs.p, t.ntrgs.p, t.n_eval_leafs, t.sbeg.p, t.tbeg.p, t.p2p_off.p,
-                  t.p2p.p,        t.center.p, t.src4.p, t.trg4.p, t.src_qim.p,    ws.out.p, f.k_re,   f.k_im};
-      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
+      NearArgs na{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.n_eval_leafs, t.sbeg.p, t.tbeg.p,
+                  t.p2p_off.p,    t.p2p.p,   t.center.p,  t.src4.p,  t.trg4.p,       t.src_qim.p, ws.out.p,
+                  f.k_re,         f.k_im,    ws.srcf.p,   t.x0[0],   t.x0[1],        t.x0[2]};
+      if constexpr (KER == K_LAPLACE && sizeof(R) == 4) {
+        if (t.nsrc > 0) {
+          k_src_split<<<nblk(t.nsrc, 256), 256, 0, s>>>(t.src4.p, t.nsrc, t.x0[0], t.x0[1], t.x0[2], ws.srcf.p);
+          XLAUNCH();
+          ws.launches++;
+        }
         k_near_lap_f2<<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
-      else
+      } else
         k_near<KER, R><<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
       XLAUNCH();
       ws.launches++;
@@ -2070,6 +2326,12 @@ void stage_times(Fmm& f, Tree& t, double* ms14) {
   Workspace* ws = t.ws[f.precision];
   XREQUIRE(ws, XFMM_ERR_STATE, "no evaluate has run");
   XCUDA(cudaEventSynchronize(ws->ev[7]));
+  int dev_status = 0;
+  XCUDA(cudaMemcpy(&dev_status, ws->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (dev_status) {
+    XCUDA(cudaMemset(ws->status.p, 0, sizeof(int)));
+    XREQUIRE(false, XFMM_ERR_TIMEOUT, "a bounded device-side wait ran out in the last pass (results incomplete)");
+  }
   auto el = [](cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
     return cudaEventElapsedTime(&ms, a, b) == cudaSuccess ? (double)ms : 0.0;

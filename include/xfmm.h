@@ -110,7 +110,8 @@ xfmm_status xfmm_tree_dump(const xfmm_tree* tree, double* geo, uint64_t* key, in
  * sub-stages forward transform, Hadamard, backward transform; the number of this library's kernel
  * launches in the last evaluate (library GEMM and FFT launches not counted); then the target
  * evaluation split into its near field (P2P) and far field (M2P + L2P) (14 doubles).  Waits for the
- * last pass to finish. */
+ * last pass to finish; XFMM_ERR_TIMEOUT when a bounded device-side wait of that pass ran out (its
+ * results are then incomplete). */
 xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms14);
 
 /* Direct near-field kernel over raw arrays: out (ntrg x 4) += potential and gradient

@@ -143,3 +143,25 @@ def test_mixed_matches_the_reference_single_precision_build(name):
     assert ours[0] <= theirs[0] and ours[1] <= theirs[1], (ours, theirs)
     diff = orc.rel_l2(out, g["out32"])  # triangle bound: within the two errors
     assert diff[0] <= 1.01 * (ours[0] + theirs[0]) and diff[1] <= 1.01 * (ours[1] + theirs[1]), (diff, ours, theirs)
+
+
+def test_hadamard_tcgen05_form(monkeypatch):
+    """The dense M2L Hadamard on tcgen05 (TMEM operands, single-thread MMA issue; chosen per workspace by
+    XFMM_HADAMARD_TCGEN05=1) against the default mma.sync form and the FP64 direct sum."""
+    import exafmm.laplace as L
+    rng = np.random.default_rng(5)
+    x = rng.random((60000, 3))
+    q = rng.uniform(-1, 1, 60000)
+    ex = orc.direct("laplace", x, q, x[:400])
+    outs = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("XFMM_HADAMARD_TCGEN05", flag)
+        fmm = L.LaplaceFmm(8, 64, precision="mixed")
+        tree = L.setup(L.init_sources(x, q), L.init_targets(x), fmm)
+        out = L.evaluate(tree, fmm)
+        fmm.stage_times(tree)  # raises if a bounded device wait ran out
+        pe, ge = orc.rel_l2(out[:400], ex)
+        assert pe < 1e-6 and ge < 3e-6, (flag, pe, ge)
+        outs.append(out)
+    pe, ge = orc.rel_l2(outs[1], outs[0])
+    assert pe < 5e-7 and ge < 5e-7, (pe, ge)
