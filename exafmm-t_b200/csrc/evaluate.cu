@@ -715,6 +715,86 @@ __global__ void __launch_bounds__(128) k_surf_pot(SurfPotArgs a) {
   }
 }
 
+// P2M check potentials of the Laplace mixed path with paired FP32: two sources per instruction
+// (__ffma2_rn etc.), 64 sources staged per chunk as float2 pairs, each lane holding SP_KB check points
+// per block.  The check surface (half-width 2.95 r) lies at least 1.95 r from every body of the leaf,
+// so no pair coincides (no r == 0 mask) and single FP32 coordinates relative to the leaf centre keep
+// the separations accurate to a few ulps.  Padding sources have zero charge.
+constexpr int SP_KB = 8;  // check points per lane per block
+struct SurfSmemF2 {
+  float4 pr[32][2];  // source pair j = sources 2j, 2j + 1: {x, x, y, y}, {z, z, q, q}
+};
+__global__ void __launch_bounds__(128) k_surf_pot_lap_f2(SurfPotArgs a) {
+  __shared__ SurfSmemF2 sm[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int w = blockIdx.x * 4 + wid;
+  if (w >= a.count) return;
+  const int node = a.nodes[w];
+  const double4 c = a.center[node];
+  const double b = a.alpha * c.w;
+  const int n = a.nsurf, ns = a.nsrcs[node];
+  const int64_t sb = a.sbeg[node];
+  float* out = (float*)a.out + (int64_t)w * n;
+  const float2 M1 = make_float2(-1.f, -1.f);
+  for (int j0 = 0; j0 < ns || j0 == 0; j0 += 64) {
+    const bool first = j0 == 0;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int j = j0 + 32 * h + lane;
+      float x = 0.f, y = 0.f, z = 0.f, q = 0.f;
+      if (j < ns) {
+        const double4 sv = a.src4[sb + j];
+        x = (float)(sv.x - c.x);
+        y = (float)(sv.y - c.y);
+        z = (float)(sv.z - c.z);
+        q = (float)sv.w;
+      }
+      float* r = reinterpret_cast<float*>(sm[wid].pr[16 * h + (lane >> 1)]) + (lane & 1);
+      r[0] = x;
+      r[2] = y;
+      r[4] = z;
+      r[6] = q;
+    }
+    __syncwarp();
+    const int npair = (min(64, max(ns - j0, 0)) + 1) >> 1;
+    for (int k0 = 0; k0 < n; k0 += 32 * SP_KB) {
+      const int nk = min(SP_KB, (n - k0 + 31) >> 5);  // slots of this block holding points (warp-uniform)
+      float2 px[SP_KB], py[SP_KB], pz[SP_KB], acc[SP_KB];
+#pragma unroll
+      for (int i = 0; i < SP_KB; i++) {
+        const int k = min(k0 + lane + 32 * i, n - 1);  // lanes past the end repeat the last point
+        px[i] = dup2((float)(a.surf_base[3 * k] * b));
+        py[i] = dup2((float)(a.surf_base[3 * k + 1] * b));
+        pz[i] = dup2((float)(a.surf_base[3 * k + 2] * b));
+        acc[i] = make_float2(0.f, 0.f);
+      }
+      for (int jp = 0; jp < npair; jp++) {
+        const float4 A = sm[wid].pr[jp][0], B = sm[wid].pr[jp][1];
+        const float2 SX = make_float2(A.x, A.y), SY = make_float2(A.z, A.w);
+        const float2 SZ = make_float2(B.x, B.y), Q = make_float2(B.z, B.w);
+#pragma unroll
+        for (int i = 0; i < SP_KB; i++) {
+          if (i >= nk) break;
+          const float2 dx = __ffma2_rn(SX, M1, px[i]), dy = __ffma2_rn(SY, M1, py[i]), dz = __ffma2_rn(SZ, M1, pz[i]);
+          float2 r2 = __fmul2_rn(dx, dx);
+          r2 = __ffma2_rn(dy, dy, r2);
+          r2 = __ffma2_rn(dz, dz, r2);
+          acc[i] = __ffma2_rn(Q, make_float2(rsqrtf(r2.x), rsqrtf(r2.y)), acc[i]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < SP_KB; i++) {
+        const int k = k0 + lane + 32 * i;
+        if (k < n) {
+          const float o = (acc[i].x + acc[i].y) * (float)INV4PI;
+          out[k] = first ? o : out[k] + o;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // ================================================================ translation GEMMs
 // Row gather / scatter around the library GEMMs: the rows of an operator application live at scattered
 // offsets (leaf and node rows of up/dn/chk/eq), the GEMMs want them contiguous.
@@ -744,6 +824,15 @@ __global__ void k_rows_scatter(int m, int n, const TS* __restrict__ src, const i
   }
 }
 inline int rows_grid(int64_t total) { return (int)std::min<int64_t>(nblk(total), 148 * 16); }
+// Columns of y = B1^T c kept for e = B2 y: the pinv rank rounded up to a multiple of 8 (at most n), so
+// that rows of y start 64-byte aligned and the library picks its aligned (tensor-core) GEMM kernels.
+// Exact: the B2 rows past the rank are zero.
+inline int pinv_cols(int rank, int n) { return std::min(n, (rank + 7) & ~7); }
+__global__ void k_to_double(const float* __restrict__ in, int64_t n, double* __restrict__ out) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = (double)in[e];
+}
+
 
 #define XCUBLAS2(call)                                                                               \
   do {                                                                                               \
@@ -773,6 +862,11 @@ inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const double2* A, con
 }
 
 // Row-major C[m][n] = A[m][k] B[k][n] with leading dimensions (rows of A, B, C lda, ldb, ldc apart).
+inline void gemm_rm_ld(cublasHandle_t h, int m, int n, int k, const float* A, int lda, const float* B, int ldb,
+                       float* C, int ldc) {
+  const float one = 1.f, zero = 0.f;
+  XCUBLAS2(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, B, ldb, A, lda, &zero, C, ldc));
+}
 inline void gemm_rm_ld(cublasHandle_t h, int m, int n, int k, const double* A, int lda, const double* B, int ldb,
                        double* C, int ldc) {
   const double one = 1.0, zero = 0.0;
@@ -1221,7 +1315,7 @@ __global__ void __launch_bounds__(HADC_NT, 4)
                   const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq,
                   int* __restrict__ status) {
   using namespace tc5;
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // B blocks need 16-byte alignment (no swizzle)
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
@@ -1971,7 +2065,10 @@ struct Engine {
     if (t.nleafs) {
       SurfPotArgs a{t.leafs.p,  t.nleafs, t.nsrcs.p,     nullptr,  t.level.p, t.sbeg.p,   nullptr, t.center.p,
                     t.src4.p,   t.src_qim.p, f.surf_base.p, n,      2.95,      ws.chk.p, 0,         f.k_re, f.k_im};
-      k_surf_pot<KER, R><<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
+      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
+        k_surf_pot_lap_f2<<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
+      else
+        k_surf_pot<KER, R><<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
       XLAUNCH();
       ws.launches++;
       W* up = (W*)ws.up.p;
@@ -1985,13 +2082,15 @@ struct Engine {
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
         const Ops<W, V64> o = ops_of<W, V64>(f, l);
-        // rows of this leaf level, contiguous in FP64; e = (V S+) (U^H c) in two FP64 GEMMs; scaled scatter
+        // rows of this leaf level, contiguous in FP64; e = (V S+) (U^H c) in two FP64 GEMMs; scaled scatter.
+        // (An FP32 first factor, as in L2P below, measured 1.4e-7 more potential error at p = 8 and 3e-7
+        // at p = 10: the upward densities feed every later translation.)
         const int64_t tot = (int64_t)m * n;
         k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.chk.p, ws.p2m1.a.p + off, nullptr,
                                                             X + (int64_t)off * n);
         XLAUNCH();
         // y = U^H c over the kept singular directions only (rank r <= n), then e = V S+ y
-        const int r = f.ops[KER == K_LAPLACE ? 0 : l].rank;
+        const int r = pinv_cols(f.ops[KER == K_LAPLACE ? 0 : l].rank, n);
         gemm_rm_ld(ws.blas, m, r, n, X + (int64_t)off * n, n, o.p2m1, n, Y + (int64_t)off * n, r);
         gemm_rm_ld(ws.blas, m, n, r, Y + (int64_t)off * n, r, o.p2m2, n, X + (int64_t)off * n, n);
         k_rows_scatter<V64, W><<<rows_grid(tot), 256, 0, s>>>(m, n, X + (int64_t)off * n, ws.p2m2.c.p + off,
@@ -2211,11 +2310,27 @@ struct Engine {
         if (m <= 0) continue;
         const Ops<W, V64> o = ops_of<W, V64>(f, l);
         const int64_t tot = (int64_t)m * n;
-        k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.dn.p, ws.l2p1.a.p + off,
-                                                            alpha_of<double>(ws.l2p2) + off, X + (int64_t)off * n);
-        XLAUNCH();
-        const int r = f.ops[KER == K_LAPLACE ? 0 : l].rank;
-        gemm_rm_ld(ws.blas, m, r, n, X + (int64_t)off * n, n, o.l2p1, n, Y + (int64_t)off * n, r);
+        const int r = pinv_cols(f.ops[KER == K_LAPLACE ? 0 : l].rank, n);
+        // The mixed path's downward check values are FP32 and conj(VH) is orthogonal: y = conj(VH) c runs
+        // in FP32 (the library's tensor-core emulation where it has it) inside this level's FP64 row block,
+        // then y moves to FP64 for e = conj(U) S+ y, whose 1/s amplification needs FP64.  These densities
+        // feed only the leaf's own targets (measured: +0.5e-7 potential error at p = 8, +1e-7 at p = 10).
+        if constexpr (sizeof(W) == 4) {
+          float* Xf = reinterpret_cast<float*>(X + (int64_t)off * n);
+          float* Yf = Xf + tot;
+          k_rows_gather<W, float><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.dn.p, ws.l2p1.a.p + off,
+                                                                alpha_of<double>(ws.l2p2) + off, Xf);
+          XLAUNCH();
+          gemm_rm_ld(ws.blas, m, r, n, Xf, n, (const float*)f.ops[KER == K_LAPLACE ? 0 : l].l2p_B1f.p, n, Yf, r);
+          k_to_double<<<rows_grid((int64_t)m * r), 256, 0, s>>>(Yf, (int64_t)m * r, Y + (int64_t)off * n);
+          XLAUNCH();
+          ws.launches++;
+        } else {
+          k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.dn.p, ws.l2p1.a.p + off,
+                                                              alpha_of<double>(ws.l2p2) + off, X + (int64_t)off * n);
+          XLAUNCH();
+          gemm_rm_ld(ws.blas, m, r, n, X + (int64_t)off * n, n, o.l2p1, n, Y + (int64_t)off * n, r);
+        }
         gemm_rm_ld(ws.blas, m, n, r, Y + (int64_t)off * n, r, o.l2p2, n, X + (int64_t)off * n, n);
         k_rows_scatter<V64, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, X + (int64_t)off * n, ws.l2p2.c.p + off,
                                                                nullptr, (V64*)ws.eq.p, 0);

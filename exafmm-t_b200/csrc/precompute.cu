@@ -370,6 +370,12 @@ void precompute(Fmm& f, int depth, cudaStream_t s) {
       dst[i]->alloc((size_t)n * n * vs * sizeof(double));
       XCUDA(cudaMemcpyAsync(dst[i]->p, F[i].p, (size_t)n * n * vs * sizeof(double), cudaMemcpyDeviceToDevice, s));
     }
+    // the mixed path's L2P first factor (an orthogonal rotation of FP32 check values) runs in FP32
+    if (single && !cplx) {
+      op.l2p_B1f.alloc((size_t)n * n * sizeof(float));
+      k_to_single<<<nb((int64_t)n * n), 256, 0, s>>>(F[2].p, (float*)op.l2p_B1f.p, (int64_t)n * n);
+      XLAUNCH();
+    }
     op.m2m_B.alloc((size_t)8 * n * n * wsz);
     op.l2l_B.alloc((size_t)8 * n * n * wsz);
     for (int c = 0; c < 8; c++) {

@@ -157,6 +157,7 @@ struct LevelOps {
   DBuf<char> p2m_B2;   // [n][n]      e = V S+ y       : B2[k][j] = conj(VH[k][j]) / s_k
   DBuf<char> l2p_B1;   // [n][n]      y = conj(VH) c   : B1[k][j] = conj(VH[j][k])
   DBuf<char> l2p_B2;   // [n][n]      e = conj(U) S+ y : B2[k][j] = conj(U[j][k]) / s_k
+  DBuf<char> l2p_B1f;  // FP32 copy of l2p_B1 (mixed path, real kernels: the L2P first factor runs in FP32)
   DBuf<char> m2m_B;    // [8n][n]     B[c*n+k][j] = M2M[c][j][k], M2M[c] = (V S+)(U^H K_c)
   DBuf<char> l2l_B;    // [n][8n]     B[k][c*n+j] = M2M[c][k][j] (L2L = M2M^T)
   DBuf<char> m2l_T;    // [26][nfreq][64] complex: entry [s*8+t] (fmm_scale_invariant.h:549-551)
