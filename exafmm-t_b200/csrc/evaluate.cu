@@ -262,6 +262,118 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_eval(EvalArgs a) {
   }
 }
 
+// Far field (M2P + L2P) of the Laplace mixed path, in FP64: the sums over equivalent densities cancel
+// strongly, so every term needs FP64.  Warp per target leaf, targets mapped to lanes as in k_eval; the
+// equivalent surfaces (each W-list node's upward surface, then the leaf's own downward surface) are
+// staged 128 points at a time as FP64 (x, y, z, density) relative to the leaf centre, and each lane runs
+// four points at once into four partial sums, so the FP64 pipe has independent work between the
+// long-latency steps.  1/r: the FP64 reciprocal-square-root approximation instruction (relative error
+// below 2^-22.9) and one Newton step (~2^-44).  No pair coincides: a target lies at least 1.95 r from
+// its own downward surface, and W-list nodes are not adjacent to the leaf.
+__device__ __forceinline__ double rsqrt_approx64(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  return y;
+}
+constexpr int FAR_CH = 128;  // surface points staged per chunk
+__device__ __forceinline__ void far_pair(double tx, double ty, double tz, const double4& s, double& p, double& gx,
+                                         double& gy, double& gz) {
+  const double dx = tx - s.x, dy = ty - s.y, dz = tz - s.z;
+  const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+  double y = rsqrt_approx64(r2);
+  y = y * fma(-0.5 * r2, y * y, 1.5);
+  const double qi = s.w * y;
+  const double qi3 = qi * (y * y);
+  p += qi;
+  gx = fma(-qi3, dx, gx);
+  gy = fma(-qi3, dy, gy);
+  gz = fma(-qi3, dz, gz);
+}
+template <class W>
+__global__ void __launch_bounds__(32 * EVAL_WARPS) k_far_lap(EvalArgs a) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int w = blockIdx.x * EVAL_WARPS + wid;
+  if (w >= a.n_eval) return;
+  __shared__ double4 sp[EVAL_WARPS][FAR_CH];
+  const int pos = a.eval_leafs[w];
+  const int node = a.leafs[pos];
+  const int T = a.ntrgs[node];
+  const int64_t tb = a.tbeg[node];
+  const double4 c = a.center[node];
+  const int n = a.nsurf;
+  const W* upv = (const W*)a.up;
+  const double* eqv = (const double*)a.eq;
+  for (int t0 = 0, Tc = 0; t0 < T; t0 += Tc) {
+    // blocks of 32 targets, the last 17..32 as 16 + the rest; 2..32 lanes per target split the points
+    Tc = T - t0 > 32 ? 32 : (T - t0 > 16 ? 16 : T - t0);
+    int G2 = 1;
+    while (G2 * 2 * Tc <= 32) G2 *= 2;
+    const int tl = lane / G2, sub = lane % G2;
+    const bool active = tl < Tc;
+    double tx = 0, ty = 0, tz = 0;
+    if (active) {
+      const double4 t = a.trg4[tb + t0 + tl];
+      tx = t.x - c.x;
+      ty = t.y - c.y;
+      tz = t.z - c.z;
+    }
+    double P[4] = {0, 0, 0, 0}, GX[4] = {0, 0, 0, 0}, GY[4] = {0, 0, 0, 0}, GZ[4] = {0, 0, 0, 0};
+    auto consume = [&](int cnt) {
+      __syncwarp();
+      if (active) {
+        int j = sub;
+        for (; j + 3 * G2 < cnt; j += 4 * G2) {
+#pragma unroll
+          for (int u = 0; u < 4; u++) far_pair(tx, ty, tz, sp[wid][j + u * G2], P[u], GX[u], GY[u], GZ[u]);
+        }
+        for (; j < cnt; j += G2) far_pair(tx, ty, tz, sp[wid][j], P[0], GX[0], GY[0], GZ[0]);
+      }
+      __syncwarp();
+    };
+    // M2P: W-list nodes' upward equivalent surfaces (1.05 box, fmm_base.h:103-121)
+    for (int64_t e = a.m2p_off[node]; e < a.m2p_off[node + 1]; e++) {
+      const int s = a.m2p[e];
+      const double4 cs = a.center[s];
+      const double b = 1.05 * cs.w;
+      for (int j0 = 0; j0 < n; j0 += FAR_CH) {
+        const int cnt = min(FAR_CH, n - j0);
+        for (int i = lane; i < cnt; i += 32) {
+          const int k = j0 + i;
+          sp[wid][i] = make_double4(cs.x + a.surf_base[3 * k] * b - c.x, cs.y + a.surf_base[3 * k + 1] * b - c.y,
+                                    cs.z + a.surf_base[3 * k + 2] * b - c.z, (double)upv[(int64_t)s * n + k]);
+        }
+        consume(cnt);
+      }
+    }
+    // L2P: own downward equivalent surface (2.95 box, fmm_scale_invariant.h:221-228)
+    const double b = 2.95 * c.w;
+    for (int j0 = 0; j0 < n; j0 += FAR_CH) {
+      const int cnt = min(FAR_CH, n - j0);
+      for (int i = lane; i < cnt; i += 32) {
+        const int k = j0 + i;
+        sp[wid][i] = make_double4(a.surf_base[3 * k] * b, a.surf_base[3 * k + 1] * b, a.surf_base[3 * k + 2] * b,
+                                  eqv[(int64_t)pos * n + k]);
+      }
+      consume(cnt);
+    }
+    double p = (P[0] + P[1]) + (P[2] + P[3]), gx = (GX[0] + GX[1]) + (GX[2] + GX[3]);
+    double gy = (GY[0] + GY[1]) + (GY[2] + GY[3]), gz = (GZ[0] + GZ[1]) + (GZ[2] + GZ[3]);
+    for (int o = 1; o < G2; o <<= 1) {
+      p += __shfl_xor_sync(0xffffffffu, p, o);
+      gx += __shfl_xor_sync(0xffffffffu, gx, o);
+      gy += __shfl_xor_sync(0xffffffffu, gy, o);
+      gz += __shfl_xor_sync(0xffffffffu, gz, o);
+    }
+    if (active && sub == 0) {
+      double* o = a.out + (tb + t0 + tl) * 4;
+      o[0] += p * INV4PI;
+      o[1] += gx * INV4PI;
+      o[2] += gy * INV4PI;
+      o[3] += gz * INV4PI;
+    }
+  }
+}
+
 // ================================================================ near field (P2P)
 // Warp per target leaf.  The sources of the leaf's P2P list form one continuous stream that is
 // staged 32 at a time in shared memory as leaf-relative coordinates (FP32: hi + lo parts, so the
@@ -2364,7 +2476,10 @@ struct Engine {
       XCUDA(cudaEventRecord(ws.ev[8], s));
       a.do_near = 0;
       a.accumulate = 1;
-      k_eval<KER, double, W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
+      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
+        k_far_lap<W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
+      else
+        k_eval<KER, double, W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
       XLAUNCH();
       ws.launches++;
     } else {
