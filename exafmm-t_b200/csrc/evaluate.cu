@@ -1620,6 +1620,10 @@ size_t ft_fwd_smem(int p) {
 template <class R>
 size_t ft_bwd_smem(int p) { return ft_fwd_smem<R>(p); }
 
+template <class CT>
+__device__ __forceinline__ CT ft_mul(CT a, CT b) {
+  return CT{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
 // w[m] = e^{sign 2 pi i m / n1} from the (cos, sin) table
 template <class CT, int N>
 __device__ __forceinline__ void ft_load_w(const double* __restrict__ tw, double sign, CT (&w)[N]) {
@@ -1670,18 +1674,23 @@ __global__ void __launch_bounds__(FT_NT, FtMinB<R>::v)
     }
   }
   __syncthreads();
-  // pass 2, along b, one column (ch, c, ka) per task: sB[(cc N + kb) H + ka] = sum_b sA[(cc P + b) H + ka] w^{kb b}
+  // pass 2, along b, one column (ch, c, ka) per task: sB[(cc N + kb) H + ka] = sum_b sA[(cc P + b) H + ka] w^{kb b}.
+  // Even and odd b summed apart: w^{(kb + P) b} = (-1)^b w^{kb b} (N = 2P), so outputs kb and kb + P are
+  // even + odd and even - odd.
   for (int e = tid; e < CPB * P * H; e += FT_NT) {
     const int ka = e % H, cc = e / H;
     CT v[P];
 #pragma unroll
     for (int b = 0; b < P; b++) v[b] = sA[(cc * P + b) * H + ka];
 #pragma unroll
-    for (int kb = 0; kb < N; kb++) {
-      CT acc = v[0];
+    for (int kb = 0; kb < P; kb++) {
+      CT ev = v[0], od = ft_mul(v[1], w[kb % N]);
 #pragma unroll
-      for (int b = 1; b < P; b++) vfma(acc, v[b], w[(kb * b) % N]);
-      sB[(cc * N + kb) * H + ka] = acc;
+      for (int b = 2; b < P; b += 2) vfma(ev, v[b], w[(kb * b) % N]);
+#pragma unroll
+      for (int b = 3; b < P; b += 2) vfma(od, v[b], w[(kb * b) % N]);
+      sB[(cc * N + kb) * H + ka] = CT{ev.x + od.x, ev.y + od.y};
+      sB[(cc * N + kb + P) * H + ka] = CT{ev.x - od.x, ev.y - od.y};
     }
   }
   __syncthreads();
@@ -1694,11 +1703,14 @@ __global__ void __launch_bounds__(FT_NT, FtMinB<R>::v)
     CT* o = spec + ((int64_t)col * ns + s) * 8 + ch0 + ch;
     const int64_t fstride = (int64_t)NC * ns * 8;
 #pragma unroll
-    for (int kc = 0; kc < N; kc++) {
-      CT acc = v[0];
+    for (int kc = 0; kc < P; kc++) {  // outputs kc and kc + P from the even and odd c sums, as in pass 2
+      CT ev = v[0], od = ft_mul(v[1], w[kc % N]);
 #pragma unroll
-      for (int c = 1; c < P; c++) vfma(acc, v[c], w[(kc * c) % N]);
-      o[kc * fstride] = acc;
+      for (int c = 2; c < P; c += 2) vfma(ev, v[c], w[(kc * c) % N]);
+#pragma unroll
+      for (int c = 3; c < P; c += 2) vfma(od, v[c], w[(kc * c) % N]);
+      o[kc * fstride] = CT{ev.x + od.x, ev.y + od.y};
+      o[(kc + P) * fstride] = CT{ev.x - od.x, ev.y - od.y};
     }
   }
 }
@@ -1719,34 +1731,46 @@ __global__ void __launch_bounds__(FT_NT, FtMinB<R>::v)
   CT w[N];
   ft_load_w(tw, 1.0, w);
   if (tid < N) sw[tid] = CT{(R)tw[2 * tid], (R)tw[2 * tid + 1]};
-  // pass A, along kc, to the outputs c = P + c', one column (ch, kb, ka) per task
+  // pass A, along kc, to the outputs c = P + c', one column (ch, kb, ka) per task.  With kc = k + P j
+  // (j = 0, 1): w^{(k + P j) m} = (-1)^{j m} w^{k m}, so output m = P + c' is the P-term sum over k of
+  // (v[k] + v[k + P]) w^{k m} for even m and (v[k] - v[k + P]) w^{k m} for odd m.
   for (int e = tid; e < NC * CPB; e += FT_NT) {
     const int ch = e % CPB, col = e / CPB;
     const CT* y = spec + ((int64_t)col * nt + t) * 8 + ch0 + ch;
     const int64_t fstride = (int64_t)NC * nt * 8;
-    CT v[N];
+    CT up[P], um[P];
 #pragma unroll
-    for (int kc = 0; kc < N; kc++) v[kc] = y[kc * fstride];
+    for (int k = 0; k < P; k++) {
+      const CT a = y[k * fstride], b = y[(k + P) * fstride];
+      up[k] = CT{a.x + b.x, a.y + b.y};
+      um[k] = CT{a.x - b.x, a.y - b.y};
+    }
 #pragma unroll
     for (int cc = 0; cc < P; cc++) {
-      CT acc = v[0];
+      const bool odd = (P + cc) & 1;
+      CT acc = odd ? um[0] : up[0];
 #pragma unroll
-      for (int kc = 1; kc < N; kc++) vfma(acc, v[kc], w[(kc * (P + cc)) % N]);
+      for (int k = 1; k < P; k++) vfma(acc, odd ? um[k] : up[k], w[(k * (P + cc)) % N]);
       sZ1[(ch * P + cc) * NC + col] = acc;
     }
   }
   __syncthreads();
   // pass B, along kb, to the outputs b = P + b', one column (ch, c', ka) per task
-  for (int e = tid; e < CPB * P * H; e += FT_NT) {
+  for (int e = tid; e < CPB * P * H; e += FT_NT) {  // same pairing of kb and kb + P as pass A
     const int ka = e % H, cc = e / H;
-    CT v[N];
+    CT up[P], um[P];
 #pragma unroll
-    for (int kb = 0; kb < N; kb++) v[kb] = sZ1[(cc * N + kb) * H + ka];
+    for (int k = 0; k < P; k++) {
+      const CT a = sZ1[(cc * N + k) * H + ka], b = sZ1[(cc * N + k + P) * H + ka];
+      up[k] = CT{a.x + b.x, a.y + b.y};
+      um[k] = CT{a.x - b.x, a.y - b.y};
+    }
 #pragma unroll
     for (int bb = 0; bb < P; bb++) {
-      CT acc = v[0];
+      const bool odd = (P + bb) & 1;
+      CT acc = odd ? um[0] : up[0];
 #pragma unroll
-      for (int kb = 1; kb < N; kb++) vfma(acc, v[kb], w[(kb * (P + bb)) % N]);
+      for (int k = 1; k < P; k++) vfma(acc, odd ? um[k] : up[k], w[(k * (P + bb)) % N]);
       sZ2[(cc * P + bb) * H + ka] = acc;
     }
   }
