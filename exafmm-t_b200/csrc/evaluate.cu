@@ -1128,7 +1128,7 @@ __global__ void __launch_bounds__(128 * HadKC<CT>::KC) k_hadamard(const CT* __re
 // are scheduled by position (k_hadamard_rt): a CTA owns HADR_TT sparse targets at one frequency, their
 // pairs are grouped by position and packed on the host into rounds of HADR_RW pairs that share one 8x8
 // block, and each pair's products are added to its output row with 16-byte vector atomics resolved in
-// L2 (the sums are taken in a run-dependent order) on rows zeroed first by k_zero_rows.
+// L2 (the sums are taken in a run-dependent order) on rows the same CTA zeroed first.
 // Spectra and products are frequency-major, (frequency f, node, child c) at [(f * nnodes + node) * 8 + c]:
 // a CTA (one frequency) reads its sources from one block of the spectra and writes its rows contiguously.
 #ifndef XFMM_HAD_DENSE_MIN
@@ -1139,16 +1139,6 @@ constexpr int HADR_NT = 256;            // threads per CTA
 constexpr int HADR_TT = 512;            // targets per tile
 constexpr int HADR_RW = 64;             // pairs per round (4 row tiles of 16)
 
-// out[f][rows[k]][0..8) = 0 for every frequency and every listed row (-1 entries skipped)
-__global__ void k_zero_rows(float2* __restrict__ out, const int* __restrict__ rows, int nrows, int ntrg, int nfreq) {
-  const int64_t total = (int64_t)nfreq * nrows * 4;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(e & 3);
-    const int64_t fr = e >> 2;
-    const int f = (int)(fr / nrows), row = rows[fr - (int64_t)f * nrows];
-    if (row >= 0) reinterpret_cast<float4*>(out + ((int64_t)f * ntrg + row) * 8)[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-}
 
 // Hadamard product, dense form on the tensor cores (FP32 accuracy from three TF32 products).
 // Per frequency the dense product is a real GEMM, D[target][16] = A[target][26 x 16] B[26 x 16][16]:
@@ -1251,11 +1241,16 @@ __global__ void __launch_bounds__(HADR_NT, 2)
   uint4* sB = reinterpret_cast<uint4*>(smem_raw);
   const int tile = blockIdx.x, f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
+  const int t0 = tile * HADR_TT;
+  float2* of = out + (int64_t)f * ntrg * 8;
+  // every product of this tile's targets at frequency f is added by this CTA: their rows start at zero
+  for (int e = tid; e < HADR_TT * 4; e += HADR_NT) {
+    const int row = rows[t0 + (e >> 2)];
+    if (row >= 0) reinterpret_cast<float4*>(of + (int64_t)row * 8)[e & 3] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   hadt_fill_b(sB, T, f, nfreq, tid, HADR_NT);
   __syncthreads();
-  const int t0 = tile * HADR_TT;
   const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + t;
-  float2* of = out + (int64_t)f * ntrg * 8;
   const int r1 = tile_r[tile + 1];
   for (int r = tile_r[tile] + wid; r < r1; r += NW) {
     const int ipos = rpos[r];
@@ -2301,9 +2296,6 @@ struct Engine {
         XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
         if (ntiles > 0) {
           const int* rows = ws.hadr_row.p + (int64_t)ws.had_tile0[g] * HADR_TT;
-          const int nrows = ntiles * HADR_TT;
-          k_zero_rows<<<rows_grid((int64_t)nfreq * nrows * 4), 256, 0, s>>>((CT*)ws.specA.p, rows, nrows, nt, nfreq);
-          XLAUNCH();
           if (!ws.hadrt_attr) {
             XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
             ws.hadrt_attr = true;
@@ -2312,7 +2304,7 @@ struct Engine {
               T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
               ws.hadr_ent.p, rows, ns, nt, nfreq);
           XLAUNCH();
-          ws.launches += 2;
+          ws.launches++;
         }
         if (ws.hadd_ld[g] > 0 && ws.had_tc5) {
           if (!ws.hadc_attr) {
