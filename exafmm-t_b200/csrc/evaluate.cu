@@ -612,11 +612,12 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
       const int nseg = (int)(e1 - eb < NEAR_SEG ? e1 - eb : NEAR_SEG);
       __syncwarp();
       int carry = 0;
+      int own_b = -1, own_e = -1;  // stream positions of the leaf's own sources in this batch
       for (int k0 = 0; k0 < nseg; k0 += 32) {
         const int k = k0 + lane;
-        int cnt = 0;
+        int cnt = 0, sn = -1;
         if (k < nseg) {
-          const int sn = a.p2p[eb + k];
+          sn = a.p2p[eb + k];
           cnt = a.nsrcs[sn];
           sm.seg_beg[k] = a.sbeg[sn];
         }
@@ -627,6 +628,12 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
           if (lane >= o) incl += v;
         }
         if (k < nseg) sm.seg_pre[k + 1] = carry + incl;
+        const unsigned om = __ballot_sync(0xffffffffu, sn == node);
+        if (om) {
+          const int l = __ffs(om) - 1;
+          own_e = carry + __shfl_sync(0xffffffffu, incl, l);
+          own_b = own_e - __shfl_sync(0xffffffffu, cnt, l);
+        }
         carry += __shfl_sync(0xffffffffu, incl, 31);
       }
       if (lane == 0) sm.seg_pre[0] = 0;
@@ -659,6 +666,9 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
         float2 p2[TPL], gx2[TPL], gy2[TPL], gz2[TPL];
 #pragma unroll
         for (int u = 0; u < TPL; u++) p2[u] = gx2[u] = gy2[u] = gz2[u] = make_float2(0.f, 0.f);
+        // r == 0 (a target meeting itself or a duplicate point; both lie in the leaf's own sources) and
+        // the zero-charge padding (the stream's last chunk) need the mask; the other chunks skip it
+        auto pairs = [&](auto masked) {
 #pragma unroll 4
         for (int jj = 0; jj < npl; jj++) {
           const int jp = jj * G2 + sub;  // source pair
@@ -677,8 +687,10 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
             r2 = __ffma2_rn(dy, dy, r2);
             r2 = __ffma2_rn(dz, dz, r2);
             float ia = rsqrtf(r2.x), ib = rsqrtf(r2.y);
-            ia = r2.x > 0.f ? ia : 0.f;  // r == 0 contributes nothing (laplace.h:57)
-            ib = r2.y > 0.f ? ib : 0.f;
+            if constexpr (decltype(masked)::value) {
+              ia = r2.x > 0.f ? ia : 0.f;  // r == 0 contributes nothing (laplace.h:57)
+              ib = r2.y > 0.f ? ib : 0.f;
+            }
             const float2 inv = make_float2(ia, ib);
             const float2 qi = __fmul2_rn(Q, inv);
             const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
@@ -688,6 +700,9 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
             gz2[u] = __ffma2_rn(qi3, dz, gz2[u]);
           }
         }
+        };
+        if (p0 + NEAR_CH > total || (own_b < p0 + NEAR_CH && own_e > p0)) pairs(std::true_type());
+        else pairs(std::false_type());
 #pragma unroll
         for (int u = 0; u < TPL; u++) {
           P[u] += (double)(p2[u].x + p2[u].y);
@@ -720,7 +735,7 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
 }
 
 #ifndef XFMM_NEARF2_MINB
-#define XFMM_NEARF2_MINB 1  // minimum resident blocks per SM requested from the register allocator
+#define XFMM_NEARF2_MINB 4  // minimum resident blocks per SM requested from the register allocator (<= 128 registers)
 #endif
 #ifndef XFMM_NEARF2_TPL
 #define XFMM_NEARF2_TPL 2  // largest number of targets per lane (2 or 4)
