@@ -1,21 +1,23 @@
 // evaluate.cu -- upward and downward passes of the KIFMM on the GPU.
 //
 // Stage map (reference -> here):
-//   P2M   fmm_scale_invariant.h:163-195 / fmm.h:156-185  k_surf_pot (check potentials) + row gather, two FP64
-//                                                        library GEMMs (pinv factors), scaled scatter (0.5^l)
+//   P2M   fmm_scale_invariant.h:163-195 / fmm.h:156-185  k_surf_pot (Laplace mixed: k_surf_pot_lap_f2) check
+//                                                        potentials + row gather, two FP64 library GEMMs
+//                                                        (pinv factors), scaled scatter (0.5^l)
 //   M2M   fmm_scale_invariant.h:233-253 / fmm.h:221-241  row gather + library GEMM per level, K = 8 nsurf
 //   P2L   fmm_base.h:127-154                             k_p2l
-//   M2L   fmm_scale_invariant.h:407-440, 560-646;        real kernels: k_m2l_fwd + k_hadamard_dt/_rt + k_m2l_bwd
-//         fmm.h:395-446, 631-788                         (FP64: k_hadamard); complex kernel or p > 10:
-//                                                        k_m2l_grid_up + cuFFT + k_transpose + Hadamard
-//                                                        + k_transpose + cuFFT + k_m2l_gather_dn
+//   M2L   fmm_scale_invariant.h:407-440, 560-646;        real kernels: k_m2l_fwd + k_hadamard_dt/_rt (opt-in:
+//         fmm.h:395-446, 631-788                         k_hadamard_dc on tcgen05) + k_m2l_bwd (FP64:
+//                                                        k_hadamard); complex kernel or p > 10: k_m2l_grid_up
+//                                                        + cuFFT + k_transpose + Hadamard + k_transpose +
+//                                                        cuFFT + k_m2l_gather_dn
 //   L2L   fmm_scale_invariant.h:256-275 / fmm.h:244-263  row gather + library GEMM per level, N = 8 nsurf
-//   L2P   fmm_scale_invariant.h:198-230 / fmm.h:188-218  scaled row gather, two FP64 library GEMMs, scatter
-//                                                        + k_eval (far part)
-//   M2P   fmm_base.h:97-124                              k_eval (far part)
-//   P2P   fmm_base.h:82-94                               k_eval (near part)
-// The near and far target evaluations share one warp-per-leaf kernel; results stay in
-// tree order until get_values scatters them (python/exafmm.cpp:194-207).
+//   L2P   fmm_scale_invariant.h:198-230 / fmm.h:188-218  scaled row gather, two library GEMMs (the mixed
+//                                                        path's first factor FP32), scatter; then the far
+//                                                        part of the target evaluation
+//   M2P   fmm_base.h:97-124                              far part: k_eval (Laplace mixed: k_far_lap)
+//   P2P   fmm_base.h:82-94                               near part: k_near (Laplace mixed: k_near_lap_f2)
+// Results stay in tree order until get_values scatters them (python/exafmm.cpp:194-207).
 #include <cublas_v2.h>
 #include <cufft.h>
 
@@ -735,7 +737,7 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
 }
 
 #ifndef XFMM_NEARF2_MINB
-#define XFMM_NEARF2_MINB 4  // minimum resident blocks per SM requested from the register allocator (<= 128 registers)
+#define XFMM_NEARF2_MINB 6  // minimum resident blocks per SM asked of the register allocator (measured best of 1..8)
 #endif
 #ifndef XFMM_NEARF2_TPL
 #define XFMM_NEARF2_TPL 2  // largest number of targets per lane (2 or 4)
