@@ -1194,13 +1194,6 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t& h, uint32_t& t) {
   h = tf32_head(x);
   t = tf32_head(x - __uint_as_float(h));
 }
-// The same split with the tail left unrounded, for operands split on every use: the tensor core reads
-// only a TF32 operand's top 19 bits, so the tail (at most 12 significant bits after a round-to-nearest
-// head) is truncated there instead, an error below 2^-22 |x| of either sign.
-__device__ __forceinline__ void tf32_split_a(float x, uint32_t& h, uint32_t& t) {
-  h = tf32_head(x);
-  t = __float_as_uint(x - __uint_as_float(h));
-}
 
 // The B fragments of frequency f for every (position, reduction step c, output half h, lane):
 // sB[(ipos * 4 + c * 2 + h) * 32 + lane] = {b0 head, b1 head, b0 tail, b1 tail}, step c covering the
@@ -1231,10 +1224,10 @@ __device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, co
 #pragma unroll
   for (int c = 0; c < 2; c++) {
     uint32_t a0h, a0t, a1h, a1t, a2h, a2t, a3h, a3t;
-    tf32_split_a(c == 0 ? x0.x : x0.z, a0h, a0t);
-    tf32_split_a(c == 0 ? x1.x : x1.z, a1h, a1t);
-    tf32_split_a(c == 0 ? x0.y : x0.w, a2h, a2t);
-    tf32_split_a(c == 0 ? x1.y : x1.w, a3h, a3t);
+    tf32_split(c == 0 ? x0.x : x0.z, a0h, a0t);
+    tf32_split(c == 0 ? x1.x : x1.z, a1h, a1t);
+    tf32_split(c == 0 ? x0.y : x0.w, a2h, a2t);
+    tf32_split(c == 0 ? x1.y : x1.w, a3h, a3t);
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       const uint4 bb = b[c * 2 + h];
@@ -1248,7 +1241,7 @@ __device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, co
 // Round form on the tensor cores (sparse targets): each round of 64 same-position pairs as 4 row tiles of
 // 16 (pair 16 j + g and 16 j + 8 + g of tile j); lanes t and t ^ 1 trade halves so each adds 16 bytes
 // (two target components of one pair) with a vector atomic.
-__global__ void __launch_bounds__(HADR_NT, 2)
+__global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 registers, a 20-byte spill)
     k_hadamard_rt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
                   const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
                   const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
@@ -1518,7 +1511,7 @@ __global__ void __launch_bounds__(HADC_NT, 4)
         const float xs[8] = {a.x, a.y, b.x, b.y, a.z, a.w, b.z, b.w};
         uint32_t ah[8], at[8];
 #pragma unroll
-        for (int i = 0; i < 8; i++) tf32_split_a(xs[i], ah[i], at[i]);
+        for (int i = 0; i < 8; i++) tf32_split(xs[i], ah[i], at[i]);
         const uint32_t ta = tw + ((uint32_t)(16 * h) << 16) + 32 * s;
         st_16x256b_x2(ta, ah);
         st_16x256b_x2(ta + 16, at);
