@@ -1039,6 +1039,11 @@ __global__ void k_transpose(const CT* __restrict__ in, CT* __restrict__ out, int
     if (r < R && c < C) out[c * R + r] = tile[threadIdx.x][i];
   }
 }
+// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away from zero: half of the 13
+// dropped bits' range is added to the magnitude and the dropped bits are cleared (a carry moves into
+// the exponent when the rounding crosses a binade).  Integer ALU work, where the conversion instruction
+// would run on the much narrower transcendental/conversion pipe.
+__device__ __forceinline__ uint32_t tf32_head(float x) { return (__float_as_uint(x) + 0x1000u) & 0xffffe000u; }
 template <class CT>
 void transpose(const CT* in, CT* out, int64_t R, int64_t C, cudaStream_t s) {
   dim3 grid((unsigned)((C + 31) / 32), (unsigned)((R + 31) / 32));
@@ -1170,19 +1175,11 @@ constexpr int HADR_RW = 64;             // pairs per round (4 row tiles of 16)
 #ifndef XFMM_HADT_TILES
 #define XFMM_HADT_TILES 4  // row tiles of 16 targets per warp
 #endif
-#ifndef XFMM_HADT_PREFETCH
-#define XFMM_HADT_PREFETCH 0  // load the next position's spectra while multiplying the current ones
-#endif
 constexpr int HADT_NT = 256;                                    // threads per CTA
 constexpr int HADT_TILES = XFMM_HADT_TILES;
 constexpr int HADT_TT = (HADT_NT / 32) * 16 * HADT_TILES;      // targets per CTA
 constexpr size_t HADT_SMEM = (size_t)26 * 4 * 32 * 16;
 
-// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away from zero: half of the 13
-// dropped bits' range is added to the magnitude and the dropped bits are cleared (a carry moves into
-// the exponent when the rounding crosses a binade).  Integer ALU work, where the conversion instruction
-// would run on the much narrower transcendental/conversion pipe.
-__device__ __forceinline__ uint32_t tf32_head(float x) { return (__float_as_uint(x) + 0x1000u) & 0xffffe000u; }
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
                                          uint32_t b1) {
   asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
@@ -1321,26 +1318,7 @@ __global__ void __launch_bounds__(HADT_NT, 2)
 #pragma unroll
       for (int i = 0; i < 4; i++) acc[j][h][i] = 0.f;
   float4 x[HADT_TILES][2];
-#if XFMM_HADT_PREFETCH
-#pragma unroll
-  for (int j = 0; j < HADT_TILES; j++)
-#pragma unroll
-    for (int r = 0; r < 2; r++) {
-      const int src = tab[base + 16 * j + 8 * r];
-      x[j][r] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#endif
   for (int ipos = 0; ipos < 26; ipos++) {
-#if XFMM_HADT_PREFETCH
-    float4 xn[HADT_TILES][2];
-#pragma unroll
-    for (int j = 0; j < HADT_TILES; j++)
-#pragma unroll
-      for (int r = 0; r < 2; r++) {
-        const int src = ipos + 1 < 26 ? tab[(ipos + 1) * ld + base + 16 * j + 8 * r] : -1;
-        xn[j][r] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-#else
 #pragma unroll
     for (int j = 0; j < HADT_TILES; j++)
 #pragma unroll
@@ -1348,7 +1326,6 @@ __global__ void __launch_bounds__(HADT_NT, 2)
         const int src = tab[ipos * ld + base + 16 * j + 8 * r];
         x[j][r] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-#endif
     uint4 b[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) b[q] = sB[(ipos * 4 + q) * 32 + lane];
@@ -1363,13 +1340,6 @@ __global__ void __launch_bounds__(HADT_NT, 2)
 #pragma unroll
         for (int i = 0; i < 4; i++) acc[j][h][i] += d[h][i];
     }
-#if XFMM_HADT_PREFETCH
-#pragma unroll
-    for (int j = 0; j < HADT_TILES; j++) {
-      x[j][0] = xn[j][0];
-      x[j][1] = xn[j][1];
-    }
-#endif
   }
   // D fragment: row g (and g + 8), columns 2t, 2t + 1 of half h = target component 4 h + t (re, im)
   float2* of = out + (int64_t)f * ntrg * 8;
@@ -1385,125 +1355,224 @@ __global__ void __launch_bounds__(HADT_NT, 2)
 }
 
 // Hadamard product, dense form on the sm_100 tensor cores through tcgen05 (FP32 accuracy from three TF32
-// products, as in k_hadamard_dt).  A CTA of 128 threads owns 128 dense targets -- thread i, target slot i
-// of the tile, TMEM lane i -- and HADC_FPB frequencies.  Per frequency the 26 positions' B blocks
-// (16 x 16 reals, TF32 head and tail) are laid out in shared memory as K-major core matrices.  Per
-// position every thread gathers its target's source spectrum (16 reals), splits it into TF32 head and
-// tail and stores both into TMEM (operand A); one thread then issues the position's six M128 N16 K8 MMAs
-// (A tail x B head, A head x B tail, A head x B head per 8-wide step) into a fresh TMEM accumulator and
-// commits them to an mbarrier.  A and D are double-buffered: the MMAs of one position run while the
-// threads gather and split the next, and each position's products are read back (tcgen05.ld) two
-// positions later and added to FP32 running sums in registers with round-to-nearest adds (the tensor
-// core's own accumulation is not rounded to nearest, so it never spans more than one position).
-// Every wait is bounded; a wait that runs out ends the CTA's work and sets *status.
-constexpr int HADC_NT = 128;
-#ifndef XFMM_HADC_FPB
-#define XFMM_HADC_FPB 2
-#endif
-constexpr int HADC_FPB = XFMM_HADC_FPB;                   // frequencies per CTA
-constexpr size_t HADC_SMEM = (size_t)26 * 2 * 1024;        // B of one frequency: [position][head, tail], 1 KB each
-constexpr uint32_t HADC_TMEM_COLS = 128;                   // A: 2 x (16 head + 16 tail) columns, D: 2 x 16 columns
-constexpr uint32_t HADC_D = 64;                            // first D column
-constexpr long long HADC_WAIT = 2000000000LL;              // SM cycles (about a second) before a wait gives up
+// products, as in k_hadamard_dt), as a warp-specialised pipeline.  A CTA owns 128 dense targets (target
+// slot i = TMEM lane i) and HADC_FPB frequencies, i.e. a stream of 26 HADC_FPB positions.
+//   * Warps 0-3 (one per TMEM lane quarter) produce and consume: per position, the 4 lanes of a quad load
+//     one source spectrum as 4 contiguous 16-byte pieces (one position ahead), split it into TF32 head
+//     and tail and store both into the position's TMEM stage (operand A, `tcgen05.st.16x256b`), then
+//     arrive on the stage's `full` barrier.  Before reusing a stage they wait for its `done` barrier,
+//     read the products of the position HADC_S earlier back (`tcgen05.ld`) and add them to FP32 running
+//     sums in registers (round-to-nearest adds; the tensor core's own accumulation never spans more than
+//     one position); after a frequency's last position they store its 128 output rows.
+//   * Warp 4 issues: per frequency one bulk copy of the 26 positions' B blocks (built once per operator
+//     in the MMA layout by k_hadc_btab) into shared memory, then per position, once the stage is full,
+//     six M128 N16 K8 kind::tf32 MMAs (A tail x B head, A head x B tail, A head x B head per 8-wide
+//     step) into the stage's fresh TMEM accumulator, committed to `done`.
+// No CTA-wide barrier inside the stream.  Every wait is bounded (about a second); a wait that runs out
+// ends the waiting role's loop, the others then run out in turn, the CTA releases its TMEM and *status
+// is set.
+constexpr int HADC_NT = 160;                                // 4 producer/consumer warps + 1 MMA warp
+constexpr int HADC_S = 4;                                   // TMEM stages
+constexpr int HADC_D = 4;                                   // positions gathered ahead (cp.async ring)
+constexpr int HADC_R = HADC_D + 1;                          // ring slots: 128 rows x 64 bytes each
+constexpr int HADC_FPB = 8;                                 // frequencies per CTA
+constexpr uint32_t HADC_BBYTES = 26 * 2048;                 // B of one frequency: [position][head, tail] 1 KB each
+// dynamic shared memory per CTA: B, then the gather ring; at least 96 KB so that at most two CTAs share an
+// SM, whose TMEM (512 columns) holds exactly two allocations of HADC_TMEM_COLS
+constexpr size_t HADC_RING = (size_t)HADC_R * 128 * 64;
+constexpr size_t HADC_SMEM = HADC_BBYTES + HADC_RING > 96 * 1024 ? HADC_BBYTES + HADC_RING : 96 * 1024;
+static_assert(3 * HADC_SMEM > 228 * 1024 && 2 * HADC_SMEM <= 227 * 1024, "two CTAs per SM");
+constexpr uint32_t HADC_TMEM_COLS = 256;                    // A: HADC_S x 32 columns, then D: HADC_S x 16
+constexpr uint32_t HADC_DCOL = 32 * HADC_S;                 // first D column
+constexpr long long HADC_WAIT = 2000000000LL;               // SM cycles (about a second) before a wait gives up
+static_assert(HADC_DCOL + 16 * HADC_S <= HADC_TMEM_COLS, "TMEM columns");
 
 // The A columns (reduction index) are a permutation of the 16 input reals fixed by the TMEM store shape
 // (16x256b): the 4 lanes of a quad load one source spectrum as 4 contiguous 16-byte pieces, lane q the
 // reals 4q .. 4q + 3, which land in columns 2q, 2q + 1, 8 + 2q, 9 + 2q.  Column of input real k:
-__device__ __forceinline__ int hadc_col(int k) {
+__host__ __device__ __forceinline__ int hadc_col(int k) {
   const int q = k >> 2, r = k & 3;
   return r < 2 ? 2 * q + r : 8 + 2 * q + (r - 2);
 }
 // byte offset of B element (output real n, A column c) in the 1 KB block of one (position, part):
 // core matrix (c / 4, n / 8) at 256 (c / 4) + 128 (n / 8), its row n % 8 at 16 (n % 8), column c % 4
-__device__ __forceinline__ uint32_t hadc_boff(int n, int c) {
+__host__ __device__ __forceinline__ uint32_t hadc_boff(int n, int c) {
   return (uint32_t)((c >> 2) * 256 + (n >> 3) * 128 + (n & 7) * 16 + (c & 3) * 4);
 }
-// lane (g, q)'s pieces of the spectra of its warp's rows g, g + 8, g + 16, g + 24 (one index per lane in idx)
-__device__ __forceinline__ void hadc_load(float4 (&x)[4], const float4* __restrict__ inf, int idx, int g, int q) {
+// btab[f] (HADC_BBYTES per frequency): factor m(sc, tc) of position ipos -> the real 2 x 2 block
+// (outputs 2 tc, 2 tc + 1; inputs 2 sc, 2 sc + 1) = [[Re m, -Im m], [Im m, Re m]], TF32 head then tail
+__global__ void k_hadc_btab(const float2* __restrict__ T, int nfreq, unsigned char* __restrict__ btab) {
+  const int64_t total = (int64_t)nfreq * 26 * 64;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int f = (int)(e / (26 * 64)), ipos = (int)(e / 64 % 26), sc = (int)(e >> 3 & 7), tc = (int)(e & 7);
+    const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + sc * 8 + tc];
+    const float v[4] = {m.x, -m.y, m.y, m.x};
+    unsigned char* blk = btab + (int64_t)f * HADC_BBYTES + ipos * 2048;
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int src = __shfl_sync(0xffffffffu, idx, g + 8 * i);
-    x[i] = src >= 0 ? __ldg(inf + (int64_t)src * 4 + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int j = 0; j < 4; j++) {
+      const uint32_t off = hadc_boff(2 * tc + (j >> 1), hadc_col(2 * sc + (j & 1)));
+      uint32_t h, t;
+      tf32_split(v[j], h, t);
+      *reinterpret_cast<uint32_t*>(blk + off) = h;
+      *reinterpret_cast<uint32_t*>(blk + 1024 + off) = t;
+    }
   }
 }
+// a bounded wait whose outcome every lane of the warp shares
+__device__ __forceinline__ bool hadc_wait(uint32_t mbar, uint32_t parity) {
+  return __all_sync(0xffffffffu, tc5::mbar_wait(mbar, parity, HADC_WAIT));
+}
 
-__global__ void __launch_bounds__(HADC_NT, 4)
-    k_hadamard_dc(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
+__global__ void __launch_bounds__(HADC_NT, 2)
+    k_hadamard_dc(const unsigned char* __restrict__ btab, const float2* __restrict__ in, float2* __restrict__ out,
                   const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq,
                   int* __restrict__ status) {
   using namespace tc5;
-  extern __shared__ __align__(16) unsigned char smem_raw[];  // B blocks need 16-byte alignment (no swizzle)
-  __shared__ __align__(8) uint64_t mbar[2];
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // B blocks of the current frequency, gather ring
+  __shared__ __align__(8) uint64_t mbar[2 * HADC_S + 2];       // full[S], done[S], B half 0, B half 1
   __shared__ uint32_t tmem_base;
-  const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, g = lane >> 2, q = lane & 3;
-  const int k = blockIdx.x * HADC_NT + tid;  // dense target slot (TMEM lane tid)
+  const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
   const uint32_t sB = smem_u32(smem_raw);
-  const uint32_t bar0 = smem_u32(&mbar[0]);  // barrier of buffer s at bar0 + 8 s
+  const uint32_t full0 = smem_u32(&mbar[0]), done0 = smem_u32(&mbar[HADC_S]), barB0 = smem_u32(&mbar[2 * HADC_S]);
   if (wid == 0) {
     tmem_alloc(smem_u32(&tmem_base), HADC_TMEM_COLS);
     tmem_relinquish();
   }
   if (tid == 0) {
-    mbar_init(bar0, 1);
-    mbar_init(bar0 + 8, 1);
+    for (int s = 0; s < HADC_S; s++) {
+      mbar_init(full0 + 8 * s, 4);
+      mbar_init(done0 + 8 * s, 1);
+    }
+    mbar_init(barB0, 1);
+    mbar_init(barB0 + 8, 1);
     fence_mbar_init();
   }
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
-  const uint32_t tm = __shfl_sync(0xffffffffu, tmem_base, 0);  // warp-uniform
-  const uint32_t tw = tm + ((uint32_t)(wid * 32) << 16);          // this warp's quarter of the lanes
-  constexpr uint32_t IDESC = idesc_tf32(128, 16);
-  const int row = rows[k];
-  uint32_t ph = 0;    // bit s: parity of the next phase of buffer s's barrier to wait for
-  uint32_t pend = 0;  // bit s: MMAs committed to buffer s's barrier and not yet waited for
+  const uint32_t tm = __shfl_sync(0xffffffffu, tmem_base, 0);
+  const int fbeg = blockIdx.y * HADC_FPB, nf = min(HADC_FPB, nfreq - fbeg);
+  const int G = 26 * nf;  // positions in this CTA's stream
   bool ok = true;
-  for (int fi = 0; fi < HADC_FPB && ok; fi++) {
-    const int f = blockIdx.y * HADC_FPB + fi;
-    if (f >= nfreq) break;
-    // B of frequency f: factor m(sc, tc) of position ipos -> the real 2 x 2 block (outputs 2 tc, 2 tc + 1;
-    // inputs 2 sc, 2 sc + 1) = [[Re m, -Im m], [Im m, Re m]], split into TF32 head (first KB) and tail
-    for (int e = tid; e < 26 * 64; e += HADC_NT) {
-      const int ipos = e >> 6, sc = (e >> 3) & 7, tc = e & 7;
-      const float2 m = T[((int64_t)ipos * nfreq + f) * 64 + sc * 8 + tc];
-      const float v[4] = {m.x, -m.y, m.y, m.x};
-      unsigned char* blk = smem_raw + ipos * 2048;
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const uint32_t off = hadc_boff(2 * tc + (j >> 1), hadc_col(2 * sc + (j & 1)));
-        uint32_t h, t;
-        tf32_split(v[j], h, t);
-        *reinterpret_cast<uint32_t*>(blk + off) = h;
-        *reinterpret_cast<uint32_t*>(blk + 1024 + off) = t;
+  if (wid == 4) {
+    // ---------------- MMA warp
+    // B in two halves (positions 0-12, 13-25), each refilled for the next frequency as soon as the MMAs
+    // that read it have completed: half 0 once position 12 is done (checked before position 12 + S, which
+    // reuses its stage), half 1 once position 25 is done (checked before the next frequency's position
+    // S - 1); frequency fi waits for half h on phase fi & 1 of its barrier.
+    constexpr uint32_t IDESC = idesc_tf32(128, 16);
+    constexpr uint32_t HB = HADC_BBYTES / 2;
+    static_assert(HADC_S <= 13 && HB % 16 == 0, "B halves");
+    auto load_half = [&](int h, int fi) {
+      if (elect_one()) {
+        mbar_arrive_expect_tx(barB0 + 8 * h, HB);
+        bulk_g2s(sB + h * HB, btab + (int64_t)(fbeg + fi) * HADC_BBYTES + h * HB, HB, barB0 + 8 * h);
       }
+      __syncwarp();
+    };
+    load_half(0, 0);
+    load_half(1, 0);
+    int issued = 0;
+    for (int gi = 0; gi < G && ok; gi++) {
+      const int fi = gi / 26, p = gi - 26 * fi, s = gi % HADC_S;
+      if (gi >= HADC_S && (p == 12 + HADC_S || p == HADC_S - 1)) {
+        // the MMAs of position gi - S (12, or the previous frequency's 25) and all before it are done:
+        // the half they read takes the next frequency's blocks
+        ok = hadc_wait(done0 + 8 * s, ((gi - HADC_S) / HADC_S) & 1);
+        if (!ok) break;
+        if (p == 12 + HADC_S && fi + 1 < nf) load_half(0, fi + 1);
+        if (p == HADC_S - 1) load_half(1, fi);
+      }
+      if (p == 0 || p == 13) {
+        ok = hadc_wait(barB0 + 8 * (p == 13), fi & 1);
+        if (!ok) break;
+      }
+      ok = hadc_wait(full0 + 8 * s, (gi / HADC_S) & 1);
+      if (!ok) break;
+      fence_after_sync();
+      if (elect_one()) {
+        const uint32_t dd = tm + HADC_DCOL + 16 * s, aa = tm + 32 * s, bb = sB + p * 2048;
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++) {
+          const uint64_t bh = sdesc_nosw(bb + 512 * kk, 256, 128), bt = sdesc_nosw(bb + 1024 + 512 * kk, 256, 128);
+          mma_tf32_ts(dd, aa + 16 + 8 * kk, bh, IDESC, kk);  // fresh sums at the first step
+          mma_tf32_ts(dd, aa + 8 * kk, bt, IDESC, 1);
+          mma_tf32_ts(dd, aa + 8 * kk, bh, IDESC, 1);
+        }
+        commit(done0 + 8 * s);
+      }
+      __syncwarp();
+      issued = gi + 1;
     }
-    fence_proxy_async_smem();
-    __syncthreads();
-    const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8);
+    // on an early end, the MMAs in flight get a bounded time to finish before the TMEM is released
+    if (!ok && issued > 0) hadc_wait(done0 + 8 * ((issued - 1) % HADC_S), ((issued - 1) / HADC_S) & 1);
+  } else {
+    // ---------------- producer / consumer warps (lane quarter wid)
+    const int g = lane >> 2, q = lane & 3;
+    const int k = blockIdx.x * 128 + tid;  // this lane's target slot = TMEM lane tid
+    const uint32_t tw = tm + ((uint32_t)(wid * 32) << 16);
+    const int row = rows[k];
     float acc[16];
 #pragma unroll
     for (int i = 0; i < 16; i++) acc[i] = 0.f;
-    float4 x[4];
-    hadc_load(x, inf, tab[k], g, q);
-    int srcn = tab[ld + k];  // this lane's row, next position
-#pragma unroll 2
-    for (int p = 0; p < 26; p++) {
-      const int s = p & 1;
-      float4 xn[4];
-      if (p + 1 < 26) hadc_load(xn, inf, srcn, g, q);
-      if (p + 2 < 26) srcn = tab[(p + 2) * ld + k];
-      if (pend >> s & 1) {  // products of position p - 2
-        ok = mbar_wait(bar0 + 8 * s, ph >> s & 1, HADC_WAIT);
-        ph ^= 1u << s;
-        pend &= ~(1u << s);
-        if (ok) {
-          fence_after_sync();
-          uint32_t d[16];
-          ld_32x32b_x16(tw + HADC_D + 16 * s, d);
-          wait_ld();
+    auto inf_of = [&](int gi) {
+      return reinterpret_cast<const float4*>(in + (int64_t)(fbeg + gi / 26) * nsrc * 8);
+    };
+    auto take = [&](int gp, int s) {  // products of stream position gp (stage s) into the sums
+      fence_after_sync();
+      uint32_t d[16];
+      ld_32x32b_x16(tw + HADC_DCOL + 16 * s, d);
+      wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; i++) acc[i] += __uint_as_float(d[i]);
+      for (int i = 0; i < 16; i++) acc[i] += __uint_as_float(d[i]);
+      if (gp % 26 == 25) {  // a frequency's last position: its rows are complete
+        if (row >= 0) {
+          float4* o = reinterpret_cast<float4*>(out + ((int64_t)(fbeg + gp / 26) * ntrg + row) * 8);
+#pragma unroll
+          for (int i = 0; i < 4; i++) o[i] = make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);
         }
+#pragma unroll
+        for (int i = 0; i < 16; i++) acc[i] = 0.f;
+      }
+    };
+    // gather ring: slot r holds, per warp and lane, the lane's 4 spectrum pieces (rows g + 8 i) of one
+    // position; each lane reads back only what it copied itself
+    const uint32_t ring = sB + HADC_BBYTES + (uint32_t)((wid * 4) * 32 + lane) * 16;
+    auto gather = [&](int gi, int idx) {  // cp.async of position gi into its slot (one commit group)
+      const float4* inf = inf_of(gi);
+      const uint32_t slot = ring + (uint32_t)(gi % HADC_R) * (128 * 64);
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int src = __shfl_sync(0xffffffffu, idx, g + 8 * i);
+        cp_async16(slot + i * 32 * 16, src >= 0 ? (const void*)(inf + (int64_t)src * 4 + q) : (const void*)in,
+                   src >= 0 ? 16u : 0u);
+      }
+      cp_async_commit();
+    };
+    // positions 0 .. D-1 in flight, the index of position D ready
+#pragma unroll
+    for (int i = 0; i < HADC_D; i++) {
+      if (i < G) gather(i, tab[(i % 26) * ld + k]);
+      else cp_async_commit();
+    }
+    int idxn = HADC_D < G ? tab[(HADC_D % 26) * ld + k] : -1;
+    for (int gi = 0; gi < G && ok; gi++) {
+      const int s = gi % HADC_S;
+      if (gi + HADC_D < G) gather(gi + HADC_D, idxn);
+      else cp_async_commit();  // keep one group per position
+      if (gi + HADC_D + 1 < G) idxn = tab[((gi + HADC_D + 1) % 26) * ld + k];
+      cp_async_wait<HADC_D>();  // position gi's group has landed
+      float4 x[4];
+      {
+        const float4* sl = reinterpret_cast<const float4*>(smem_raw + HADC_BBYTES + (size_t)(gi % HADC_R) * (128 * 64)) +
+                           (wid * 4) * 32 + lane;
+#pragma unroll
+        for (int i = 0; i < 4; i++) x[i] = sl[i * 32];
+      }
+      if (gi >= HADC_S) {  // the stage's previous position is done: take its products, then reuse it
+        ok = hadc_wait(done0 + 8 * s, ((gi - HADC_S) / HADC_S) & 1);
+        if (!ok) break;
+        take(gi - HADC_S, s);
       }
 #pragma unroll
       for (int h = 0; h < 2; h++) {  // rows 16 h + g (x[2h]) and 16 h + g + 8 (x[2h + 1]) of the warp
@@ -1518,64 +1587,24 @@ __global__ void __launch_bounds__(HADC_NT, 4)
       }
       wait_st();
       fence_before_sync();
-      if (!__syncthreads_and(ok)) {
-        ok = false;
-        break;
-      }
-      if (wid == 0) {
-        fence_after_sync();
-        if (elect_one()) {
-          const uint32_t dd = tm + HADC_D + 16 * s, aa = tm + 32 * s, bb = sB + p * 2048;
-#pragma unroll
-          for (int kk = 0; kk < 2; kk++) {
-            const uint64_t bh = sdesc_nosw(bb + 512 * kk, 256, 128), bt = sdesc_nosw(bb + 1024 + 512 * kk, 256, 128);
-            mma_tf32_ts(dd, aa + 16 + 8 * kk, bh, IDESC, kk);  // fresh sums at the first step
-            mma_tf32_ts(dd, aa + 8 * kk, bt, IDESC, 1);
-            mma_tf32_ts(dd, aa + 8 * kk, bh, IDESC, 1);
-          }
-          commit(bar0 + 8 * s);
-        }
-        __syncwarp();
-      }
-      pend |= 1u << s;
-#pragma unroll
-      for (int i = 0; i < 4; i++) x[i] = xn[i];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(full0 + 8 * s);
     }
-    // the last two positions' products
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-      if (!ok || !(pend >> s & 1)) continue;
-      ok = mbar_wait(bar0 + 8 * s, ph >> s & 1, HADC_WAIT);
-      ph ^= 1u << s;
-      pend &= ~(1u << s);
-      if (ok) {
-        fence_after_sync();
-        uint32_t d[16];
-        ld_32x32b_x16(tw + HADC_D + 16 * s, d);
-        wait_ld();
-#pragma unroll
-        for (int i = 0; i < 16; i++) acc[i] += __uint_as_float(d[i]);
-      }
+    cp_async_wait<0>();
+    for (int gp = max(G - HADC_S, 0); gp < G && ok; gp++) {  // the last positions' products
+      const int s = gp % HADC_S;
+      ok = hadc_wait(done0 + 8 * s, (gp / HADC_S) & 1);
+      if (!ok) break;
+      take(gp, s);
     }
-    if (ok && row >= 0) {
-      float4* o = reinterpret_cast<float4*>(out + ((int64_t)f * ntrg + row) * 8);
-#pragma unroll
-      for (int i = 0; i < 4; i++) o[i] = make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);
-    }
-    fence_before_sync();
-    ok = __syncthreads_and(ok);  // every thread done with this frequency's B and D before the next fill
-    fence_after_sync();
   }
-  // on an early end, give the MMAs still in flight a bounded time to finish before the TMEM is released
-  for (int s = 0; s < 2; s++)
-    if (pend >> s & 1) mbar_wait(bar0 + 8 * s, ph >> s & 1, HADC_WAIT);
   fence_before_sync();
   __syncthreads();
   if (wid == 0) {
     fence_after_sync();
     tmem_dealloc(tm, HADC_TMEM_COLS);
   }
-  if (!ok && tid == 0) atomicExch(status, 1);
+  if (!ok && lane == 0) atomicExch(status, 1);
 }
 
 // ---------------------------------------------------------------- M2L transforms of the real kernels
@@ -1894,6 +1923,9 @@ struct Workspace {
   // dense Hadamard targets on tcgen05 (k_hadamard_dc) instead of mma.sync (k_hadamard_dt): chosen when the
   // workspace is created, by XFMM_HADAMARD_TCGEN05=1 in the environment
   bool had_tc5 = false;
+  DBuf<unsigned char> hadc_btab;      // its B blocks per frequency (k_hadc_btab), built for one operator table
+  const void* hadc_btab_T = nullptr;
+  int hadc_btab_nf = 0;
   // M2L transforms: own pruned DFT kernels (real kernels, shared memory permitting) or cuFFT on the grid
   bool fused = false;
   size_t ft_fwd_smem = 0, ft_bwd_smem = 0;
@@ -2321,8 +2353,17 @@ struct Engine {
             XCUDA(cudaFuncSetAttribute(k_hadamard_dc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADC_SMEM));
             ws.hadc_attr = true;
           }
-          k_hadamard_dc<<<dim3(ws.hadd_ld[g] / HADC_NT, (nfreq + HADC_FPB - 1) / HADC_FPB), HADC_NT, HADC_SMEM, s>>>(
-              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+          if (ws.hadc_btab_T != (const void*)T || ws.hadc_btab_nf != nfreq) {  // B blocks in the MMA layout
+            ws.hadc_btab.reserve((size_t)nfreq * HADC_BBYTES);
+            k_hadc_btab<<<std::min<int64_t>(nblk((int64_t)nfreq * 26 * 64), 148 * 16), 256, 0, s>>>(T, nfreq,
+                                                                                                  ws.hadc_btab.p);
+            XLAUNCH();
+            ws.launches++;
+            ws.hadc_btab_T = T;
+            ws.hadc_btab_nf = nfreq;
+          }
+          k_hadamard_dc<<<dim3(ws.hadd_ld[g] / 128, (nfreq + HADC_FPB - 1) / HADC_FPB), HADC_NT, HADC_SMEM, s>>>(
+              ws.hadc_btab.p, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
               ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq, ws.status.p);
           XLAUNCH();
           ws.launches++;

@@ -97,6 +97,16 @@ __device__ __forceinline__ uint64_t sdesc_nosw(uint32_t saddr, uint32_t lbo, uin
          (1ull << 46);
 }
 
+// ---- per-thread asynchronous global -> shared copies of 16 bytes (src_bytes 0: the 16 bytes are zeroed)
+__device__ __forceinline__ void cp_async16(uint32_t dst_smem, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst_smem), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {  // at most N of this thread's groups still in flight
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // ---- mbarrier
 __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
@@ -111,11 +121,38 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(mbar) : "memory");
+}
+// one arrival that also expects `bytes` of asynchronous copies to complete on this phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(mbar),
+               "r"(bytes)
+               : "memory");
+}
+// bulk copy global -> this CTA's shared memory (no multicast); both addresses 16-byte aligned, bytes a
+// multiple of 16; completion is counted in bytes on the mbarrier
+__device__ __forceinline__ void bulk_g2s(uint32_t dst_smem, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_smem),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+// try_wait that lets the hardware suspend the thread until the phase completes or about `ns` pass
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t mbar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
 // Waits for the phase of the given parity to complete, for at most `limit` SM clock cycles; false if it
-// did not complete in time.
+// did not complete in time.  Each try suspends the thread (up to a millisecond) instead of spinning.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit) {
+  if (mbar_try_wait(mbar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_try_wait(mbar, parity))
+  while (!mbar_try_wait_sleep(mbar, parity, 1000000u))
     if (clock64() - t0 > limit) return false;
   return true;
 }
