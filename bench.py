@@ -253,9 +253,11 @@ def accuracy(outs, x, q):
     return {k: dict(zip(("potential", "gradient"), orc.rel_l2(v[samp], ex))) for k, v in outs.items()}
 
 
-# DRAM bytes per launch of the dominant kernel from an ncu capture of this workload (summarised under
-# profiles/, with the command); None until captured.
-NEAR_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) per launch of the dominant kernel, from an ncu capture of the same workload
+# at N = 500,000 (35.06 MB per launch), scaled to the 4M launch by its pair count (x 8.58): traffic grows
+# with the bodies streamed, which grow with the pairs at fixed density.  Capture and command:
+# profiles/near_traffic_laplace_500k_p8_mixed.md.
+NEAR_TRAFFIC_BYTES = 300_700_000
 
 
 def roofline(r, peaks, src):
