@@ -1238,7 +1238,7 @@ __device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, co
 // Round form on the tensor cores (sparse targets): each round of 64 same-position pairs as 4 row tiles of
 // 16 (pair 16 j + g and 16 j + 8 + g of tile j); lanes t and t ^ 1 trade halves so each adds 16 bytes
 // (two target components of one pair) with a vector atomic.
-__global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 registers, a 20-byte spill)
+__global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 registers, a 16-byte spill)
     k_hadamard_rt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
                   const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
                   const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
@@ -1259,14 +1259,8 @@ __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 
   __syncthreads();
   const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + t;
   const int r1 = tile_r[tile + 1];
-  for (int r = tile_r[tile] + wid; r < r1; r += NW) {
-    const int ipos = rpos[r];
-    uint4 b[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) b[q] = sB[(ipos * 4 + q) * 32 + lane];
-    // the round's pairs and their spectra first (all loads in flight), then the 4 tiles
-    int2 ee[4][2];
-    float4 xx[4][2];
+  // a round's pairs (source, output row) and their spectra, all loads in flight at once
+  auto load_round = [&](int r, int2 (&ee)[4][2], float4 (&xx)[4][2]) {
 #pragma unroll
     for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -1276,6 +1270,15 @@ __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 
 #pragma unroll
       for (int rr = 0; rr < 2; rr++)
         xx[j][rr] = ee[j][rr].x >= 0 ? __ldg(inf + (int64_t)ee[j][rr].x * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+  };
+  for (int r = tile_r[tile] + wid; r < r1; r += NW) {
+    const int ipos = rpos[r];
+    uint4 b[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = sB[(ipos * 4 + q) * 32 + lane];
+    int2 ee[4][2];
+    float4 xx[4][2];
+    load_round(r, ee, xx);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       float d[2][4];
@@ -1288,8 +1291,7 @@ __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 
         const float2 send = odd ? make_float2(d[h][0], d[h][1]) : make_float2(d[h][2], d[h][3]);
         const float rx = __shfl_xor_sync(0xffffffffu, send.x, 1), ry = __shfl_xor_sync(0xffffffffu, send.y, 1);
         const float4 v = odd ? make_float4(rx, ry, d[h][2], d[h][3]) : make_float4(d[h][0], d[h][1], rx, ry);
-        if (e.x >= 0)
-          atomicAdd(reinterpret_cast<float4*>(of + (int64_t)rows[t0 + e.y] * 8 + 4 * h + (t & ~1)), v);
+        if (e.x >= 0) atomicAdd(reinterpret_cast<float4*>(of + (int64_t)e.y * 8 + 4 * h + (t & ~1)), v);
       }
     }
   }
@@ -2089,7 +2091,7 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   if (f.mixed()) {
     // Targets with at least HAD_DENSE_MIN occupied positions go to the dense form, in tiles of HADT_TT
     // (table [26][ld], padded with -1).  The others go to the round form: tiles of HADR_TT targets;
-    // per tile and relative position the pairs (source index, target index within the tile) in rounds
+    // per tile and relative position the pairs (source index, output row) in rounds
     // of HADR_RW, padded with source -1.  Both write disjoint rows of the group's output.
     std::vector<int> tile_r, pos, srow, dtab, drow;
     std::vector<int2> ent;
@@ -2132,7 +2134,7 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
               pos.push_back(ipos);
               ent.resize(ent.size() + HADR_RW, make_int2(-1, 0));
             }
-            ent[ent.size() - HADR_RW + n] = make_int2(sidx, (int)(k - k0));
+            ent[ent.size() - HADR_RW + n] = make_int2(sidx, sparse[k] - tb);  // source, output row
             if (++n == HADR_RW) n = 0;
           }
         }
