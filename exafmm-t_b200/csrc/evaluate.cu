@@ -1320,12 +1320,18 @@ __global__ void __launch_bounds__(HADT_NT, 2)
 #pragma unroll
       for (int i = 0; i < 4; i++) acc[j][h][i] = 0.f;
   float4 x[HADT_TILES][2];
+  int srcn[HADT_TILES][2];  // source indices of the next position, loaded one position ahead
+#pragma unroll
+  for (int j = 0; j < HADT_TILES; j++)
+#pragma unroll
+    for (int r = 0; r < 2; r++) srcn[j][r] = tab[base + 16 * j + 8 * r];
   for (int ipos = 0; ipos < 26; ipos++) {
 #pragma unroll
     for (int j = 0; j < HADT_TILES; j++)
 #pragma unroll
       for (int r = 0; r < 2; r++) {
-        const int src = tab[ipos * ld + base + 16 * j + 8 * r];
+        const int src = srcn[j][r];
+        if (ipos + 1 < 26) srcn[j][r] = tab[(ipos + 1) * ld + base + 16 * j + 8 * r];
         x[j][r] = src >= 0 ? __ldg(inf + (int64_t)src * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
     uint4 b[4];
