@@ -292,6 +292,10 @@ xfmm_status xfmm_tree_dump(const xfmm_tree* tree, double* geo, uint64_t* key, in
   });
 }
 
+xfmm_status xfmm_selftest_bounded_wait(int64_t limit_cycles) {
+  return guarded([&] { xfmm::selftest_bounded_wait(limit_cycles); });
+}
+
 xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms14) {
   return guarded([&] {
     XREQUIRE(fmm && tree && ms14, XFMM_ERR_ARG, "null argument");

@@ -2627,6 +2627,34 @@ void downward_pass(Fmm& f, Tree& t, cudaStream_t s) {
 
 // Device times of the last upward + downward pass (ms): 0 P2M, 1 M2M, 2 P2L, 3 M2L, 4 L2L,
 // 5 L2P check->equivalent, 6 target evaluation (P2P + M2P + L2P), 7 total, 8-10 M2L FFT / Hadamard / iFFT.
+namespace {
+// An mbarrier (expecting one arrival) whose phase nothing completes; the wait runs out after `limit`
+// cycles and the kernel reports it through *status, as the pipelined kernels do.
+__global__ void k_selftest_wait(long long limit, int* status) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t b = tc5::smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    tc5::mbar_init(b, 1);
+    tc5::fence_mbar_init();
+  }
+  __syncthreads();
+  const bool ok = __all_sync(0xffffffffu, tc5::mbar_wait(b, 0, limit));
+  if (!ok && threadIdx.x == 0) atomicExch(status, 1);
+}
+}  // namespace
+
+void selftest_bounded_wait(int64_t limit_cycles) {
+  XREQUIRE(limit_cycles >= 1 && limit_cycles <= 1000000000LL, XFMM_ERR_ARG, "limit_cycles outside 1..1e9");
+  DBuf<int> status(1);
+  XCUDA(cudaMemset(status.p, 0, sizeof(int)));
+  k_selftest_wait<<<1, 32>>>(limit_cycles, status.p);
+  XLAUNCH();
+  XCUDA(cudaDeviceSynchronize());
+  int h = 0;
+  XCUDA(cudaMemcpy(&h, status.p, sizeof(int), cudaMemcpyDeviceToHost));
+  XREQUIRE(!h, XFMM_ERR_TIMEOUT, "bounded device-side wait ran out (self-test)");
+}
+
 void stage_times(Fmm& f, Tree& t, double* ms14) {
   Workspace* ws = t.ws[f.precision];
   XREQUIRE(ws, XFMM_ERR_STATE, "no evaluate has run");

@@ -199,6 +199,7 @@ void upward_pass(Fmm& fmm, Tree& t, cudaStream_t s);
 void downward_pass(Fmm& fmm, Tree& t, cudaStream_t s);
 void get_values(Fmm& fmm, Tree& t, double* out_dev, cudaStream_t s);
 void stage_times(Fmm& fmm, Tree& t, double* ms14);
+void selftest_bounded_wait(int64_t limit_cycles);
 void gradient_p2p_raw(int kernel, double k_re, double k_im, int precision, const double* src, int64_t ns,
                       const double* q, const double* trg, int64_t nt, double* out, cudaStream_t s);
 void verify(Fmm& fmm, Tree& t, int sample, double* err2, cudaStream_t s);

@@ -42,6 +42,7 @@ SIGNATURES = [
     ("xfmm_gradient_p2p", i32, [i32, f64, f64, i32, vp, i64, vp, vp, i64, vp, i32, vp]),
     ("xfmm_verify", i32, [vp, vp, i32, vp, vp]),
     ("xfmm_gradient_p2p_noalloc", i32, [i32, f64, f64, i32, vp, i64, vp, vp, i64, vp, vp]),
+    ("xfmm_selftest_bounded_wait", i32, [i64]),
 ]
 
 

@@ -136,6 +136,12 @@ xfmm_status xfmm_gradient_p2p_noalloc(int kernel, double k_re, double k_im, int 
                                       int64_t nsrc, const double* q, const double* trg_xyz, int64_t ntrg,
                                       double* out, void* stream);
 
+/* Self-test of the bounded device-side waits (no counterpart in the reference): one kernel waits on an
+ * mbarrier phase that nothing completes, with a limit of limit_cycles SM clock cycles (1..1e9), then
+ * gives up as the library's waiting kernels do.  Returns XFMM_ERR_TIMEOUT when the wait ran out and was
+ * reported through the device status flag as designed; the device stays usable afterwards. */
+xfmm_status xfmm_selftest_bounded_wait(int64_t limit_cycles);
+
 /* FmmBase::verify on the device: relative L2 error of potential and gradient of the last
  * evaluate against FP64 direct summation over all sources, on every target (sample == 0)
  * or the targets of 10 leaves at stride nleafs/10 (sample != 0). */
