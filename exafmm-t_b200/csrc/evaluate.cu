@@ -2115,6 +2115,10 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
         for (int ipos = 0; ipos < 26; ipos++) cnt += t.h_m2l_tab[26 * (size_t)tt + ipos] >= 0;
         (cnt >= HAD_DENSE_MIN ? dense : sparse).push_back(tt);
       }
+      // dense targets level by level (node order within a level is Morton order): the targets of one
+      // tile are then spatially compact and share most of their sources in L2
+      std::stable_sort(dense.begin(), dense.end(),
+                       [&](int a, int b) { return t.h_level[t.h_m2l_trg[a]] < t.h_level[t.h_m2l_trg[b]]; });
       const int ld = (int)((dense.size() + HADT_TT - 1) / HADT_TT) * HADT_TT;
       W.hadd_ld[g] = ld;
       W.hadd_tab0[g] = (int64_t)dtab.size();

@@ -915,6 +915,7 @@ void m2l_setup(Fmm& fmm, Tree& t, cudaStream_t s) {
   t.n_m2l_trg = (int)trg.size();
   t.m2l_src.upload(src, s);
   t.m2l_trg.upload(trg, s);
+  t.h_m2l_trg = trg;
   t.m2l_tab.upload(tab, s);
   t.h_m2l_tab = tab;
   t.m2l_scale.upload(scale, s);

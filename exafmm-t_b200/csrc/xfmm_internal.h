@@ -137,6 +137,7 @@ struct Tree {
   DBuf<int> m2l_src;                  // compact source list (node idx), grouped by level if per-level
   std::vector<int> m2l_src_off;       // group offsets
   DBuf<int> m2l_trg;                  // targets (nonleaf node idx), same grouping
+  std::vector<int> h_m2l_trg;         // host copy
   std::vector<int> m2l_trg_off;
   DBuf<int> m2l_tab;                  // [n_trg][26] compact source index within its group, -1 if none
   std::vector<int> h_m2l_tab;
