@@ -170,7 +170,6 @@ xfmm_status xfmm_precompute(xfmm_fmm* fmm, xfmm_tree* tree, void* stream) {
 xfmm_status xfmm_set_charges(xfmm_fmm* fmm, xfmm_tree* tree, const double* q, int on_device, void* stream) {
   return guarded([&] {
     XREQUIRE(fmm && tree && q, XFMM_ERR_ARG, "null argument");
-    if (!on_device) check_finite_host(q, (size_t)tree->t.nsrc * (fmm->f.is_complex() ? 2 : 1), "charges");
     xfmm::set_charges(fmm->f, tree->t, q, on_device != 0, S(stream));
   });
 }

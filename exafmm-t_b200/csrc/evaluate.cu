@@ -1160,6 +1160,10 @@ constexpr int HAD_DENSE_MIN = XFMM_HAD_DENSE_MIN;  // occupied positions that ma
 constexpr int HADR_NT = 256;            // threads per CTA
 constexpr int HADR_TT = 512;            // targets per tile
 constexpr int HADR_RW = 64;             // pairs per round (4 row tiles of 16)
+#ifndef XFMM_HADR_TPC
+#define XFMM_HADR_TPC 4
+#endif
+constexpr int HADR_TPC = XFMM_HADR_TPC;  // tiles per CTA (one B fill per frequency for all of them)
 
 
 // Hadamard product, dense form on the tensor cores (FP32 accuracy from three TF32 products).
@@ -1177,7 +1181,11 @@ constexpr int HADR_RW = 64;             // pairs per round (4 row tiles of 16)
 #endif
 constexpr int HADT_NT = 256;                                    // threads per CTA
 constexpr int HADT_TILES = XFMM_HADT_TILES;
-constexpr int HADT_TT = (HADT_NT / 32) * 16 * HADT_TILES;      // targets per CTA
+constexpr int HADT_TT = (HADT_NT / 32) * 16 * HADT_TILES;      // targets per CTA tile
+#ifndef XFMM_HADT_TPC
+#define XFMM_HADT_TPC 1
+#endif
+constexpr int HADT_TPC = XFMM_HADT_TPC;                         // CTA tiles per CTA (one B fill for all)
 constexpr size_t HADT_SMEM = (size_t)26 * 4 * 32 * 16;
 
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
@@ -1241,24 +1249,25 @@ __device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, co
 __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 registers, a 16-byte spill)
     k_hadamard_rt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
                   const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
-                  const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
+                  const int* __restrict__ rows, int ntiles, int nsrc, int ntrg, int nfreq) {
   constexpr int NW = HADR_NT / 32;
   static_assert(HADR_RW == 64, "a round is 4 row tiles of 16 pairs");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint4* sB = reinterpret_cast<uint4*>(smem_raw);
-  const int tile = blockIdx.x, f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int t0 = tile * HADR_TT;
+  // tiles [tb, te) share this CTA's B fragments of frequency f
+  const int tb = blockIdx.x * HADR_TPC, te = min(ntiles, tb + HADR_TPC);
   float2* of = out + (int64_t)f * ntrg * 8;
-  // every product of this tile's targets at frequency f is added by this CTA: their rows start at zero
-  for (int e = tid; e < HADR_TT * 4; e += HADR_NT) {
-    const int row = rows[t0 + (e >> 2)];
+  // every product of these tiles' targets at frequency f is added by this CTA: their rows start at zero
+  for (int e = tid; e < (te - tb) * HADR_TT * 4; e += HADR_NT) {
+    const int row = rows[tb * HADR_TT + (e >> 2)];
     if (row >= 0) reinterpret_cast<float4*>(of + (int64_t)row * 8)[e & 3] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   hadt_fill_b(sB, T, f, nfreq, tid, HADR_NT);
   __syncthreads();
   const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + t;
-  const int r1 = tile_r[tile + 1];
+  const int r1 = tile_r[te];
   // a round's pairs (source, output row) and their spectra, all loads in flight at once
   auto load_round = [&](int r, int2 (&ee)[4][2], float4 (&xx)[4][2]) {
 #pragma unroll
@@ -1271,7 +1280,7 @@ __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 
       for (int rr = 0; rr < 2; rr++)
         xx[j][rr] = ee[j][rr].x >= 0 ? __ldg(inf + (int64_t)ee[j][rr].x * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
   };
-  for (int r = tile_r[tile] + wid; r < r1; r += NW) {
+  for (int r = tile_r[tb] + wid; r < r1; r += NW) {
     const int ipos = rpos[r];
     uint4 b[4];
 #pragma unroll
@@ -1310,8 +1319,10 @@ __global__ void __launch_bounds__(HADT_NT, 2)
   hadt_fill_b(sB, T, f, nfreq, tid, HADT_NT);
   __syncthreads();
   const int g = lane >> 2, t = lane & 3;
-  const int base = blockIdx.x * HADT_TT + wid * 16 * HADT_TILES + g;  // tile j, rows g / g + 8: base + 16 j (+ 8)
   const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + t;
+  // CTA tiles [blockIdx.x * HADT_TPC, ...) of HADT_TT targets share this CTA's B fragments of frequency f
+  for (int ct = blockIdx.x * HADT_TPC; ct < min(ld / HADT_TT, (blockIdx.x + 1) * HADT_TPC); ct++) {
+  const int base = ct * HADT_TT + wid * 16 * HADT_TILES + g;  // tile j, rows g / g + 8: base + 16 j (+ 8)
   float acc[HADT_TILES][2][4];
 #pragma unroll
   for (int j = 0; j < HADT_TILES; j++)
@@ -1360,6 +1371,7 @@ __global__ void __launch_bounds__(HADT_NT, 2)
 #pragma unroll
       for (int h = 0; h < 2; h++) of[(int64_t)row * 8 + 4 * h + t] = make_float2(acc[j][h][2 * r], acc[j][h][2 * r + 1]);
     }
+  }
 }
 
 // Hadamard product, dense form on the sm_100 tensor cores through tcgen05 (FP32 accuracy from three TF32
@@ -1865,6 +1877,13 @@ __global__ void k_src_split(const double4* __restrict__ src4, int64_t n, double 
   srcf[2 * i] = make_float4(hx, hy, hz, (float)v.w);
   srcf[2 * i + 1] = make_float4((float)(dx - (double)hx), (float)(dy - (double)hy), (float)(dz - (double)hz), 0.f);
 }
+// *bad becomes nonzero if any of v[0, n) is NaN or infinite
+__global__ void k_count_nonfinite(const double* __restrict__ v, int64_t n, int* __restrict__ bad) {
+  int found = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    found |= !isfinite(v[i]);
+  if (__syncthreads_or(found) && threadIdx.x == 0) atomicOr(bad, 1);
+}
 __global__ void k_set_charges(const double* __restrict__ q, const int* __restrict__ perm, int64_t n, int cplx,
                               double4* __restrict__ src4, double* __restrict__ qim) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -2354,9 +2373,9 @@ struct Engine {
             XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
             ws.hadrt_attr = true;
           }
-          k_hadamard_rt<<<dim3(ntiles, nfreq), HADR_NT, HADT_SMEM, s>>>(
+          k_hadamard_rt<<<dim3((ntiles + HADR_TPC - 1) / HADR_TPC, nfreq), HADR_NT, HADT_SMEM, s>>>(
               T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
-              ws.hadr_ent.p, rows, ns, nt, nfreq);
+              ws.hadr_ent.p, rows, ntiles, ns, nt, nfreq);
           XLAUNCH();
           ws.launches++;
         }
@@ -2384,7 +2403,7 @@ struct Engine {
             XCUDA(cudaFuncSetAttribute(k_hadamard_dt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
             ws.hadt_attr = true;
           }
-          k_hadamard_dt<<<dim3(ws.hadd_ld[g] / HADT_TT, nfreq), HADT_NT, HADT_SMEM, s>>>(
+          k_hadamard_dt<<<dim3((ws.hadd_ld[g] / HADT_TT + HADT_TPC - 1) / HADT_TPC, nfreq), HADT_NT, HADT_SMEM, s>>>(
               T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
               ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
           XLAUNCH();
@@ -2602,12 +2621,23 @@ void set_charges(Fmm& f, Tree& t, const double* q, bool on_device, cudaStream_t 
   const int vs = f.is_complex() ? 2 : 1;
   const double* dq = q;
   if (!on_device) {
-    t.stage_q.upload(q, n * vs, s);  // grow-only staging buffer owned by the tree
+    // host charges: copied to a grow-only staging buffer owned by the tree and checked there for
+    // non-finite values before any of them replaces the current charges; the call returns once the
+    // caller's buffer has been read
+    t.stage_q.upload(q, n * vs, s);
     dq = t.stage_q.p;
+    t.stage_flag.reserve(1);
+    XCUDA(cudaMemsetAsync(t.stage_flag.p, 0, sizeof(int), s));
+    k_count_nonfinite<<<std::max<int64_t>(1, std::min<int64_t>(nblk(n * vs), 4 * 148)), 256, 0, s>>>(
+        dq, n * vs, t.stage_flag.p);
+    XLAUNCH();
+    int bad = 0;
+    XCUDA(cudaMemcpyAsync(&bad, t.stage_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    XCUDA(cudaStreamSynchronize(s));
+    if (bad) throw Error(XFMM_ERR_NUMERIC, "non-finite value in charges");
   }
   k_set_charges<<<nblk(n), 256, 0, s>>>(dq, t.src_perm.p, n, f.is_complex(), t.src4.p, t.src_qim.p);
   XLAUNCH();
-  if (!on_device) XCUDA(cudaStreamSynchronize(s));
 }
 
 void clear_values(Fmm& f, Tree& t, cudaStream_t s) {

@@ -146,6 +146,7 @@ struct Tree {
   int n_m2l_src = 0, n_m2l_trg = 0;
   // persistent staging for host-side charges and results (no allocation per call)
   DBuf<double> stage_q, stage_out;
+  DBuf<int> stage_flag;               // non-finite charges found by the device-side check
 };
 
 // Precomputed operators of one level (or the single scale-invariant level).

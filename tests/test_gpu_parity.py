@@ -111,6 +111,19 @@ def test_update_charges_and_reevaluate():
     assert np.allclose(out2, 2.0 * out1, rtol=1e-12, atol=1e-12 * np.abs(out1).max())
 
 
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_update_charges_rejects_non_finite_and_keeps_the_old_charges(bad):
+    g = load("laplace_cube_p4")
+    m, fmm, tree = _setup(g, "fp64")
+    out1 = m.evaluate(tree, fmm)
+    q = g["q"].copy()
+    q[len(q) // 2] = bad
+    with pytest.raises(RuntimeError, match="non-finite value in charges"):
+        m.update_charges(tree, q)
+    out2 = m.evaluate(tree, fmm)
+    assert np.array_equal(out1, out2)
+
+
 def test_verify_matches_oracle():
     g = load("laplace_cube_p4")
     m, fmm, tree = _setup(g, "fp64")
