@@ -264,7 +264,10 @@ void precompute(Fmm& f, int depth, cudaStream_t s) {
   const int vs = cplx ? 2 : 1;        // doubles per value
   const bool single = f.mixed();
   const size_t wsz = (single ? sizeof(float) : sizeof(double)) * vs;  // bytes per working value
-  const double eps = single ? 1e-10 : 1e-16;
+#ifndef XFMM_PINV_EPS_MIXED
+#define XFMM_PINV_EPS_MIXED 1e-10
+#endif
+  const double eps = single ? XFMM_PINV_EPS_MIXED : 1e-16;
   const double r0 = f.r0;
   Handles H;
   XCUBLAS(cublasCreate(&H.blas));
