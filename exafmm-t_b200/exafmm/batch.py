@@ -8,6 +8,14 @@ single launch; ``evaluate_each`` runs the same calls one system after another wi
 Charges are read from ``charges[i]`` (device tensors) at every replay, so new values are picked up
 by writing into those tensors in place.  The work runs on the batch's own stream, ordered after the
 caller's current stream, which in turn waits for it: results may be read on the current stream.
+
+Inside the graph the systems may run concurrently: ``capture(nstreams)`` forks the batch stream into
+``nstreams`` streams (each system's calls stay in order on one of them; systems are dealt, largest
+first, to the stream with the fewest bodies so far) and joins them again, so the small grids of small
+systems share the GPU instead of running one after another.  Every system owns its operators, tree,
+work buffers and library handles (cuBLAS with a fixed workspace), so nothing is shared between the
+streams.  ``autotune()`` captures the graph for each candidate stream count, times replays on the
+device and keeps the fastest.
 """
 import ctypes
 
@@ -37,14 +45,44 @@ class BatchedFmm:
             self.outs.append(torch.zeros((len(coords), width), dtype=torch.float64, device="cuda"))
         self.n = [len(c) for c, _ in systems]
         self.stream = torch.cuda.Stream()
+        self._side = []
         self.graph = None
+        self.nstreams = 1
+        self.tuning = {}
 
-    def _enqueue(self, stream_handle):
+    def _enqueue(self, stream_handle, order=None):
         L = _lib.lib()
         st = ctypes.c_void_p(stream_handle)
-        for fmm, tree, q, out in zip(self.fmms, self.trees, self.charges, self.outs):
+        for i in (range(len(self.n)) if order is None else order):
+            fmm, tree, q, out = self.fmms[i], self.trees[i], self.charges[i], self.outs[i]
             _lib.check(L.xfmm_set_charges(fmm._h, tree._h, ctypes.c_void_p(q.data_ptr()), 1, st))
             _lib.check(L.xfmm_evaluate(fmm._h, tree._h, ctypes.c_void_p(out.data_ptr()), 1, st))
+
+    def _deal(self, nstreams):
+        """Systems per stream: largest first, each to the stream with the fewest bodies so far."""
+        load, lists = [0] * nstreams, [[] for _ in range(nstreams)]
+        for i in sorted(range(len(self.n)), key=lambda i: -self.n[i]):
+            k = min(range(nstreams), key=lambda k: load[k])
+            lists[k].append(i)
+            load[k] += self.n[i]
+        return [l for l in lists if l]
+
+    def _enqueue_forked(self, nstreams):
+        """All systems on nstreams streams forked from and joined back into the batch stream."""
+        if nstreams <= 1:
+            self._enqueue(self.stream.cuda_stream)
+            return
+        while len(self._side) < nstreams:
+            self._side.append(torch.cuda.Stream())
+        fork = torch.cuda.Event()
+        fork.record(self.stream)
+        for k, order in enumerate(self._deal(nstreams)):
+            side = self._side[k]
+            side.wait_event(fork)
+            self._enqueue(side.cuda_stream, order)
+            join = torch.cuda.Event()
+            join.record(side)
+            self.stream.wait_event(join)
 
     def evaluate_each(self):
         """One evaluate per system, launched one after another on the batch stream (no graph)."""
@@ -54,16 +92,47 @@ class BatchedFmm:
         torch.cuda.current_stream().wait_stream(self.stream)
         return self.outs
 
-    def capture(self):
-        """Capture one evaluate of every system into a CUDA graph.  The first evaluate of each system
-        (which sizes its work buffers) runs here, before the capture begins."""
+    def capture(self, nstreams=1):
+        """Capture one evaluate of every system into a CUDA graph, the systems spread over nstreams
+        concurrent streams.  The first evaluate of each system (which sizes its work buffers) runs
+        here, before the capture begins."""
         self.evaluate_each()
         self.stream.synchronize()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=self.stream):
-            self._enqueue(self.stream.cuda_stream)
+            self._enqueue_forked(int(nstreams))
         self.graph = g
+        self.nstreams = int(nstreams)
         return g
+
+    def autotune(self, candidates=(1, 2, 4, 8, 16, 32), reps=3):
+        """Capture the graph for each stream count in candidates, time `reps` replays of each on the
+        device (after one untimed replay) and keep the fastest graph.  self.tuning maps each stream
+        count to its milliseconds per replay."""
+        best = None
+        for ns in candidates:
+            ns = max(1, min(int(ns), len(self.n)))
+            if ns in self.tuning:
+                continue
+            g = self.capture(ns)
+            self.replay()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
+            for _ in range(reps):
+                with torch.cuda.stream(self.stream):
+                    g.replay()
+            e1.record(self.stream)
+            e1.synchronize()
+            self.tuning[ns] = e0.elapsed_time(e1) / reps
+            if best is None or self.tuning[ns] < self.tuning[best[0]]:
+                best = (ns, g)
+            else:
+                del g
+        if best is not None:
+            self.nstreams, self.graph = best
+        else:  # every candidate timed before: recapture the fastest
+            self.capture(min(self.tuning, key=self.tuning.get))
+        return self.nstreams
 
     def replay(self):
         """All systems in one graph launch (capture() first)."""

@@ -27,6 +27,30 @@ def test_graph_replay_equals_one_by_one_fp64():
         assert torch.equal(a, c)
 
 
+def test_graph_on_concurrent_streams_equals_one_by_one_fp64():
+    systems, b = _batch("fp64")
+    seq = [o.clone() for o in b.evaluate_each()]
+    b.capture(nstreams=3)
+    for o in b.outs:
+        o.zero_()
+    rep = b.replay()
+    torch.cuda.synchronize()
+    for a, c in zip(seq, rep):
+        assert torch.equal(a, c)
+
+
+def test_autotune_keeps_a_timed_stream_count():
+    systems, b = _batch("fp64")
+    seq = [o.clone() for o in b.evaluate_each()]
+    ns = b.autotune(candidates=(1, 2, 4), reps=2)
+    assert ns in (1, 2, 4) and set(b.tuning) == {1, 2, 4}
+    assert b.tuning[ns] == min(b.tuning.values())
+    rep = b.replay()
+    torch.cuda.synchronize()
+    for a, c in zip(seq, rep):
+        assert torch.equal(a, c)
+
+
 def test_graph_follows_charges_written_in_place():
     systems, b = _batch("mixed")
     b.capture()
