@@ -74,3 +74,4 @@ def test_batched_systems_match_direct_sums():
         s = rng.choice(len(x), 200, replace=False)
         pe, ge = orc.rel_l2(o.cpu().numpy()[s], orc.direct("laplace", x, q, x[s]))
         assert pe < 1e-4 and ge < 1e-3, (pe, ge)
+
