@@ -1850,6 +1850,242 @@ __global__ void __launch_bounds__(FT_NT, FtMinB<R>::v)
   }
 }
 
+// ---------------------------------------------------------------- M2L transforms of the complex kernel
+// The Helmholtz kernel's transforms are full complex DFTs of the n1^3 grid (forward factor
+// e^{-2 pi i k n / n1}, backward e^{+...}, both unnormalised; frequency f = (kc n1 + kb) n1 + ka): the
+// C2C transforms of the reference's FFTW plans (fmm.h:631-788).  They are pruned as the real ones are
+// (input corner [0, p)^3, output corner [p, 2p)^3; three passes of direct sums in shared memory, outputs
+// k and k + p of a length-p input from even and odd partial sums).
+constexpr int FTC_PMAX = 12;
+template <class F>
+void ftc_dispatch(int p, F&& fn) {
+  switch (p) {
+    case 2: fn(std::integral_constant<int, 2>()); break;
+    case 3: fn(std::integral_constant<int, 3>()); break;
+    case 4: fn(std::integral_constant<int, 4>()); break;
+    case 5: fn(std::integral_constant<int, 5>()); break;
+    case 6: fn(std::integral_constant<int, 6>()); break;
+    case 7: fn(std::integral_constant<int, 7>()); break;
+    case 8: fn(std::integral_constant<int, 8>()); break;
+    case 9: fn(std::integral_constant<int, 9>()); break;
+    case 10: fn(std::integral_constant<int, 10>()); break;
+    case 11: fn(std::integral_constant<int, 11>()); break;
+    case 12: fn(std::integral_constant<int, 12>()); break;
+    default: throw Error(XFMM_ERR_UNSUPPORTED, "complex M2L transform kernels cover 2 <= p <= 12");
+  }
+}
+// y[k] for k < 2P from x[0..P): y[k] = sum_m x[m] w^{k m}, w[j] = e^{sign 2 pi i j / 2P}; outputs k and
+// k + P are even + odd and even - odd (w^{(k + P) m} = (-1)^m w^{k m}); out(k, value) stores one output
+template <int P, class CT, class Out>
+__device__ __forceinline__ void ftc_dft_p(const CT (&x)[P], const CT (&w)[2 * P], Out&& out) {
+  constexpr int N = 2 * P;
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    CT ev = x[0], od = ft_mul(x[1], w[k % N]);
+#pragma unroll
+    for (int m = 2; m < P; m += 2) vfma(ev, x[m], w[(k * m) % N]);
+#pragma unroll
+    for (int m = 3; m < P; m += 2) vfma(od, x[m], w[(k * m) % N]);
+    out(k, CT{ev.x + od.x, ev.y + od.y});
+    out(k + P, CT{ev.x - od.x, ev.y - od.y});
+  }
+}
+// y[P + j] for j < P from X[0..2P): y[P + j] = sum_k X[k] w^{k (P + j)}; with k = k' + P i,
+// w^{(k' + P i)(P + j)} = (-1)^{i (P + j)} w^{k' (P + j)}: a P-term sum of X[k'] +- X[k' + P]
+template <int P, class CT, class Out>
+__device__ __forceinline__ void ftc_idft_upper(const CT (&up)[P], const CT (&um)[P], const CT (&w)[2 * P],
+                                               Out&& out) {
+  constexpr int N = 2 * P;
+#pragma unroll
+  for (int j = 0; j < P; j++) {
+    const bool odd = (P + j) & 1;
+    CT acc = odd ? um[0] : up[0];
+#pragma unroll
+    for (int k = 1; k < P; k++) vfma(acc, odd ? um[k] : up[k], w[(k * (P + j)) % N]);
+    out(j, acc);
+  }
+}
+
+// Children per CTA of the complex forward transform: the spectrum values of one frequency of all 8
+// children of a node are one 64-byte (float2) or 128-byte (double2) row, written by consecutive lanes.
+template <class R> struct FtcCpb;
+template <> struct FtcCpb<float> { static constexpr int v = 8; };
+template <> struct FtcCpb<double> { static constexpr int v = 4; };
+#ifndef XFMM_FTC_JS
+#define XFMM_FTC_JS 3
+#endif
+constexpr int FTC_JS = XFMM_FTC_JS;  // first-axis base frequencies j per slab: outputs ka = j and j + p
+template <class R>
+size_t ftc_fwd_smem(int p) {  // per child and slab: [p][p][2 JS] + [p][n1][2 JS] complex values
+  return sizeof(typename C2<R>::type) * FtcCpb<R>::v * (size_t)p * (p + 2 * p) * 2 * FTC_JS;
+}
+template <class R>
+size_t ftc_bwd_smem(int p) { return ftc_fwd_smem<R>(p); }  // [p][n1][2 JS] + [p][p][2 JS] per child
+
+// spec[(f*ns + s)*8 + child] = forward complex DFT of the children ch0 .. ch0 + CPB - 1 of source node
+// src[s].  The first-axis frequencies ka are taken in slabs (base frequencies j0 .. j0 + JS - 1 and their
+// partners j + p); per slab the three passes run on the slab's columns only, and the grid input is read
+// through the grid -> surface map (values outside the surface are zero) from the L1-resident rows of up.
+template <class R, int P>
+__global__ void __launch_bounds__(FT_NT, 1)
+    k_m2l_fwd_c(const int* __restrict__ src, int ns, const int* __restrict__ child0,
+                const typename C2<R>::type* __restrict__ up, int nsurf, const int* __restrict__ conv2surf,
+                const double* __restrict__ tw, typename C2<R>::type* __restrict__ spec) {
+  using CT = typename C2<R>::type;
+  constexpr int N = 2 * P, CPB = FtcCpb<R>::v, KS = 2 * FTC_JS;
+  const int s = blockIdx.x, ch0 = blockIdx.y * CPB, tid = threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* sA = reinterpret_cast<CT*>(smem_raw);  // [c < P][b < P][ch][slot < KS]
+  CT* sB = sA + P * P * CPB * KS;            // [c < P][kb < N][ch][slot]
+  __shared__ int sidx[P * P * P];            // grid corner [c][b][a] -> surface index or -1
+  __shared__ CT sw[N];                       // w[m] for run-time m (pass 1: the same m in every lane)
+  CT w[N];
+  ft_load_w(tw, -1.0, w);
+  if (tid < N) sw[tid] = CT{(R)tw[2 * tid], (R)(-tw[2 * tid + 1])};
+  for (int e = tid; e < P * P * P; e += FT_NT) {
+    const int a = e % P, b = (e / P) % P, c = e / (P * P);
+    sidx[e] = conv2surf[(c * N + b) * N + a];
+  }
+  const int64_t node0 = (int64_t)child0[src[s]] + ch0;
+  const int64_t fstride = (int64_t)N * N * ns * 8;
+  for (int j0 = 0; j0 < P; j0 += FTC_JS) {
+    __syncthreads();  // sidx and sw ready; the previous slab's sA / sB reads done
+    // pass 1, along a: task (c, b, ch); slots 2 q and 2 q + 1 hold ka = j0 + q and j0 + q + P
+    for (int e = tid; e < P * P * CPB; e += FT_NT) {
+      const int ch = e % CPB, cb = e / CPB;
+      const CT* u = up + (node0 + ch) * nsurf;
+      CT x[P];
+#pragma unroll
+      for (int a = 0; a < P; a++) {
+        const int k = sidx[cb * P + a];
+        x[a] = k >= 0 ? __ldg(u + k) : CT{(R)0, (R)0};
+      }
+#pragma unroll
+      for (int q = 0; q < FTC_JS; q++) {
+        const int j = j0 + q;
+        if (j >= P) break;
+        CT ev = x[0], od{(R)0, (R)0};
+#pragma unroll
+        for (int a = 1; a < P; a++) vfma(a & 1 ? od : ev, x[a], sw[(j * a) % N]);  // j known at run time only
+        sA[(cb * CPB + ch) * KS + 2 * q] = CT{ev.x + od.x, ev.y + od.y};
+        sA[(cb * CPB + ch) * KS + 2 * q + 1] = CT{ev.x - od.x, ev.y - od.y};
+      }
+    }
+    __syncthreads();
+    // pass 2, along b: task (c, ch, slot)
+    for (int e = tid; e < P * CPB * KS; e += FT_NT) {
+      const int sl = e % KS, ch = (e / KS) % CPB, c = e / (KS * CPB);
+      CT x[P];
+#pragma unroll
+      for (int b = 0; b < P; b++) x[b] = sA[((c * P + b) * CPB + ch) * KS + sl];
+      ftc_dft_p<P>(x, w, [&](int kb, CT v) { sB[((c * N + kb) * CPB + ch) * KS + sl] = v; });
+    }
+    __syncthreads();
+    // pass 3, along c: task (kb, slot, ch), children fastest: the CPB children of one frequency are
+    // written by consecutive lanes
+    for (int e = tid; e < N * KS * CPB; e += FT_NT) {
+      const int ch = e % CPB, sl = (e / CPB) % KS, kb = e / (CPB * KS);
+      const int j = j0 + sl / 2;
+      if (j >= P) continue;
+      const int ka = j + (sl & 1) * P;
+      CT x[P];
+#pragma unroll
+      for (int c = 0; c < P; c++) x[c] = sB[((c * N + kb) * CPB + ch) * KS + sl];
+      CT* o = spec + ((int64_t)(kb * N + ka) * ns + s) * 8 + ch0 + ch;
+      ftc_dft_p<P>(x, w, [&](int kc, CT v) { o[kc * fstride] = v; });
+    }
+  }
+}
+
+// dn[child ch0 + ch of target trg[t]][k] += scale[t] * backward complex DFT of spec[.][t][child] at map_dn[k],
+// for the CPB children ch0 .. of the CTA.  The first-axis frequencies ka are taken in slabs as in the
+// forward transform: per slab, pass A (along kc, rows of CPB children read by consecutive lanes) and
+// pass B (along kb) run on the slab's columns, and pass C adds the slab's terms of the last sum (along
+// ka) to per-point sums kept in registers (point i of the thread: k = tid + i FT_NT over CPB nsurf).
+template <class R, int P>
+__global__ void __launch_bounds__(FT_NT, 1)
+    k_m2l_bwd_c(const int* __restrict__ trg, int nt, const int* __restrict__ child0,
+                const typename C2<R>::type* __restrict__ spec, int nsurf, const int* __restrict__ map_dn,
+                const double* __restrict__ tw, const R* __restrict__ scale, typename C2<R>::type* __restrict__ dn) {
+  using CT = typename C2<R>::type;
+  constexpr int N = 2 * P, CPB = FtcCpb<R>::v, KS = 2 * FTC_JS;
+  constexpr int NPT = (CPB * (6 * (P - 1) * (P - 1) + 2) + FT_NT - 1) / FT_NT;  // points per thread
+  const int t = blockIdx.x, ch0 = blockIdx.y * CPB, tid = threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* sZ1 = reinterpret_cast<CT*>(smem_raw);  // [c' < P][kb < N][ch][slot < KS]
+  CT* sZ2 = sZ1 + P * N * CPB * KS;           // [c' < P][b' < P][ch][slot]
+  __shared__ CT sw[N];
+  CT w[N];
+  ft_load_w(tw, 1.0, w);
+  if (tid < N) sw[tid] = CT{(R)tw[2 * tid], (R)tw[2 * tid + 1]};
+  CT acc[NPT];
+#pragma unroll
+  for (int i = 0; i < NPT; i++) acc[i] = CT{(R)0, (R)0};
+  const int64_t fstride = (int64_t)N * N * nt * 8;
+  for (int j0 = 0; j0 < P; j0 += FTC_JS) {
+    __syncthreads();  // sw ready; the previous slab's sZ2 reads done
+    // pass A, along kc, to c = P + c': task (kb, slot, ch), children fastest (one row per frequency)
+    for (int e = tid; e < N * KS * CPB; e += FT_NT) {
+      const int ch = e % CPB, sl = (e / CPB) % KS, kb = e / (CPB * KS);
+      const int j = j0 + sl / 2;
+      if (j >= P) continue;
+      const int ka = j + (sl & 1) * P;
+      const CT* y = spec + ((int64_t)(kb * N + ka) * nt + t) * 8 + ch0 + ch;
+      CT up[P], um[P];
+#pragma unroll
+      for (int k = 0; k < P; k++) {
+        const CT a = y[k * fstride], b = y[(k + P) * fstride];
+        up[k] = CT{a.x + b.x, a.y + b.y};
+        um[k] = CT{a.x - b.x, a.y - b.y};
+      }
+      ftc_idft_upper<P>(up, um, w, [&](int cc, CT v) { sZ1[((cc * N + kb) * CPB + ch) * KS + sl] = v; });
+    }
+    __syncthreads();
+    // pass B, along kb, to b = P + b': task (c', ch, slot)
+    for (int e = tid; e < P * CPB * KS; e += FT_NT) {
+      const int sl = e % KS, ch = (e / KS) % CPB, cc = e / (KS * CPB);
+      if (j0 + sl / 2 >= P) continue;
+      CT up[P], um[P];
+#pragma unroll
+      for (int k = 0; k < P; k++) {
+        const CT a = sZ1[((cc * N + k) * CPB + ch) * KS + sl], b = sZ1[((cc * N + k + P) * CPB + ch) * KS + sl];
+        up[k] = CT{a.x + b.x, a.y + b.y};
+        um[k] = CT{a.x - b.x, a.y - b.y};
+      }
+      ftc_idft_upper<P>(up, um, w, [&](int bb, CT v) { sZ2[((cc * P + bb) * CPB + ch) * KS + sl] = v; });
+    }
+    __syncthreads();
+    // pass C, this slab's terms of the sum along ka at each point: (Z[j] + (-1)^a Z[j + P]) w^{j a}
+#pragma unroll
+    for (int i = 0; i < NPT; i++) {
+      const int e = tid + i * FT_NT;
+      if (e < CPB * nsurf) {
+        const int ch = e / nsurf, k = e - ch * nsurf, g = map_dn[k];
+        const int a = g % N, b = g / N % N - P, c = g / (N * N) - P;
+        const CT* z = sZ2 + ((c * P + b) * CPB + ch) * KS;
+        const R sgn = (a & 1) ? (R)-1 : (R)1;
+#pragma unroll
+        for (int q = 0; q < FTC_JS; q++) {
+          const int jj = j0 + q;
+          if (jj >= P) break;
+          const CT v{z[2 * q].x + sgn * z[2 * q + 1].x, z[2 * q].y + sgn * z[2 * q + 1].y};
+          vfma(acc[i], v, sw[(jj * a) % N]);
+        }
+      }
+    }
+  }
+  const int64_t node0 = (int64_t)child0[trg[t]] + ch0;
+  const R sc = scale[t];
+#pragma unroll
+  for (int i = 0; i < NPT; i++) {
+    const int e = tid + i * FT_NT;
+    if (e < CPB * nsurf) {
+      CT* d = dn + node0 * nsurf + e;  // child ch0 + e / nsurf, point e % nsurf
+      *d = CT{d->x + sc * acc[i].x, d->y + sc * acc[i].y};
+    }
+  }
+}
+
 // dn[child c of target t][k] += scale[t] * grid[(t*8 + c)*nconv + map_dn[k]]   (fmm_scale_invariant.h:639-643)
 template <class W, class RB>
 __global__ void k_m2l_gather_dn(const int* __restrict__ trg, int ntrg, const int* __restrict__ child0,
@@ -2091,7 +2327,9 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
     constexpr size_t kMaxSmem = 227 * 1024;
     const size_t fw = f.mixed() ? ft_fwd_smem<float>(f.p) : ft_fwd_smem<double>(f.p);
     const size_t bw = f.mixed() ? ft_bwd_smem<float>(f.p) : ft_bwd_smem<double>(f.p);
-    W.fused = !cplx && f.p <= FT_PMAX && fw <= kMaxSmem && bw <= kMaxSmem;
+    const size_t cw = std::max(f.mixed() ? ftc_fwd_smem<float>(f.p) : ftc_fwd_smem<double>(f.p),
+                               f.mixed() ? ftc_bwd_smem<float>(f.p) : ftc_bwd_smem<double>(f.p));
+    W.fused = cplx ? (f.p <= FTC_PMAX && cw <= kMaxSmem) : (f.p <= FT_PMAX && fw <= kMaxSmem && bw <= kMaxSmem);
   }
   W.specA.alloc((size_t)maxn * 8 * f.nfreq * 2 * rsz);
   W.specB.alloc((size_t)maxn * 8 * f.nfreq * 2 * rsz);
@@ -2351,6 +2589,19 @@ struct Engine {
           XLAUNCH();
           ws.launches++;
         }
+      } else if (ws.fused) {
+        ftc_dispatch(f.p, [&](auto pc) {
+          constexpr int PP = decltype(pc)::value;
+          const size_t smem = ftc_fwd_smem<R>(PP);
+          if (ws.ft_fwd_smem < smem) {
+            XCUDA(cudaFuncSetAttribute(k_m2l_fwd_c<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            ws.ft_fwd_smem = smem;
+          }
+          k_m2l_fwd_c<R, PP><<<dim3(ns, 8 / FtcCpb<R>::v), FT_NT, smem, s>>>(
+              src, ns, t.child0.p, (const CT*)ws.up.p, n, f.conv_to_surf_up.p, f.dft_tw.p, (CT*)ws.specB.p);
+        });
+        XLAUNCH();
+        ws.launches++;
       }
       if (!ws.fused) {
         k_m2l_grid_up<W><<<std::min<int64_t>(nblk((int64_t)ns * 8 * nconv), 148 * 32), 256, 0, s>>>(
@@ -2441,6 +2692,20 @@ struct Engine {
           XLAUNCH();
           ws.launches++;
         }
+      } else if (ws.fused) {
+        ftc_dispatch(f.p, [&](auto pc) {
+          constexpr int PP = decltype(pc)::value;
+          const size_t smem = ftc_bwd_smem<R>(PP);
+          if (ws.ft_bwd_smem < smem) {
+            XCUDA(cudaFuncSetAttribute(k_m2l_bwd_c<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            ws.ft_bwd_smem = smem;
+          }
+          k_m2l_bwd_c<R, PP><<<dim3(nt, 8 / FtcCpb<R>::v), FT_NT, smem, s>>>(trg, nt, t.child0.p, (const CT*)ws.specA.p, n,
+                                                             f.map_dn.p, f.dft_tw.p,
+                                                             m2l_scale_of<R>(t) + t.m2l_trg_off[g], (CT*)ws.dn.p);
+        });
+        XLAUNCH();
+        ws.launches++;
       }
       if (!ws.fused) {
         ws.launches++;
