@@ -8,9 +8,10 @@
 //   P2L   fmm_base.h:127-154                             k_p2l
 //   M2L   fmm_scale_invariant.h:407-440, 560-646;        real kernels: k_m2l_fwd + k_hadamard_dt/_rt (opt-in:
 //         fmm.h:395-446, 631-788                         k_hadamard_dc on tcgen05) + k_m2l_bwd (FP64:
-//                                                        k_hadamard); complex kernel or p > 10: k_m2l_grid_up
-//                                                        + cuFFT + k_transpose + Hadamard + k_transpose +
-//                                                        cuFFT + k_m2l_gather_dn
+//                                                        k_hadamard); complex kernel (p <= 12): k_m2l_fwd_c
+//                                                        + Hadamard + k_m2l_bwd_c; real p > 10 or p > 12:
+//                                                        k_m2l_grid_up + cuFFT + k_transpose + Hadamard +
+//                                                        k_transpose + cuFFT + k_m2l_gather_dn
 //   L2L   fmm_scale_invariant.h:256-275 / fmm.h:244-263  row gather + library GEMM per level, N = 8 nsurf
 //   L2P   fmm_scale_invariant.h:198-230 / fmm.h:188-218  scaled row gather, two library GEMMs (the mixed
 //                                                        path's first factor FP32), scatter; then the far
@@ -2189,7 +2190,8 @@ struct Workspace {
   DBuf<unsigned char> hadc_btab;      // its B blocks per frequency (k_hadc_btab), built for one operator table
   const void* hadc_btab_T = nullptr;
   int hadc_btab_nf = 0;
-  // M2L transforms: own pruned DFT kernels (real kernels, shared memory permitting) or cuFFT on the grid
+  // M2L transforms: own pruned DFT kernels (real p <= 10, complex p <= 12, shared memory permitting) or
+  // cuFFT on the grid
   bool fused = false;
   size_t ft_fwd_smem = 0, ft_bwd_smem = 0;
   int64_t launches = 0;  // kernels of this library launched by the last evaluate
