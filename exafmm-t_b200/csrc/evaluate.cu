@@ -1893,9 +1893,8 @@ __device__ __forceinline__ void ftc_dft_p(const CT (&x)[P], const CT (&w)[2 * P]
 }
 // y[P + j] for j < P from X[0..2P): y[P + j] = sum_k X[k] w^{k (P + j)}; with k = k' + P i,
 // w^{(k' + P i)(P + j)} = (-1)^{i (P + j)} w^{k' (P + j)}: a P-term sum of X[k'] +- X[k' + P]
-template <int P, class CT, class Out>
-__device__ __forceinline__ void ftc_idft_upper(const CT (&up)[P], const CT (&um)[P], const CT (&w)[2 * P],
-                                               Out&& out) {
+template <int P, class CT, class WT, class Out>
+__device__ __forceinline__ void ftc_idft_upper(const CT (&up)[P], const CT (&um)[P], const WT& w, Out&& out) {
   constexpr int N = 2 * P;
 #pragma unroll
   for (int j = 0; j < P; j++) {
@@ -1920,8 +1919,17 @@ template <class R>
 size_t ftc_fwd_smem(int p) {  // per child and slab: [p][p][2 JS] + [p][n1][2 JS] complex values
   return sizeof(typename C2<R>::type) * FtcCpb<R>::v * (size_t)p * (p + 2 * p) * 2 * FTC_JS;
 }
+#ifndef XFMM_FTC_JSB
+#define XFMM_FTC_JSB 2
+#endif
+constexpr int FTC_JSB = XFMM_FTC_JSB;  // base frequencies per slab of the backward transform
+// per CTA: [p][n1][CPB][2 JSB] + [p][p] rows of CPB 2 JSB + 1 (odd: the point-indexed reads of pass C
+// fall on different banks) complex values
 template <class R>
-size_t ftc_bwd_smem(int p) { return ftc_fwd_smem<R>(p); }  // [p][n1][2 JS] + [p][p][2 JS] per child
+size_t ftc_bwd_smem(int p) {
+  constexpr int ZS = FtcCpb<R>::v * 2 * FTC_JSB;
+  return sizeof(typename C2<R>::type) * ((size_t)p * 2 * p * ZS + (size_t)p * p * (ZS + 1));
+}
 
 // spec[(f*ns + s)*8 + child] = forward complex DFT of the children ch0 .. ch0 + CPB - 1 of source node
 // src[s].  The first-axis frequencies ka are taken in slabs (base frequencies j0 .. j0 + JS - 1 and their
@@ -2003,27 +2011,28 @@ __global__ void __launch_bounds__(FT_NT, 1)
 // forward transform: per slab, pass A (along kc, rows of CPB children read by consecutive lanes) and
 // pass B (along kb) run on the slab's columns, and pass C adds the slab's terms of the last sum (along
 // ka) to per-point sums kept in registers (point i of the thread: k = tid + i FT_NT over CPB nsurf).
+template <class R> struct FtcMinB;  // resident CTAs per SM of the backward transform (registers)
+template <> struct FtcMinB<float> { static constexpr int v = 2; };
+template <> struct FtcMinB<double> { static constexpr int v = 1; };
 template <class R, int P>
-__global__ void __launch_bounds__(FT_NT, 1)
+__global__ void __launch_bounds__(FT_NT, FtcMinB<R>::v)
     k_m2l_bwd_c(const int* __restrict__ trg, int nt, const int* __restrict__ child0,
                 const typename C2<R>::type* __restrict__ spec, int nsurf, const int* __restrict__ map_dn,
                 const double* __restrict__ tw, const R* __restrict__ scale, typename C2<R>::type* __restrict__ dn) {
   using CT = typename C2<R>::type;
-  constexpr int N = 2 * P, CPB = FtcCpb<R>::v, KS = 2 * FTC_JS;
+  constexpr int N = 2 * P, CPB = FtcCpb<R>::v, JS = FTC_JSB, KS = 2 * JS, ZS = CPB * KS + 1;
   constexpr int NPT = (CPB * (6 * (P - 1) * (P - 1) + 2) + FT_NT - 1) / FT_NT;  // points per thread
   const int t = blockIdx.x, ch0 = blockIdx.y * CPB, tid = threadIdx.x;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CT* sZ1 = reinterpret_cast<CT*>(smem_raw);  // [c' < P][kb < N][ch][slot < KS]
-  CT* sZ2 = sZ1 + P * N * CPB * KS;           // [c' < P][b' < P][ch][slot]
-  __shared__ CT sw[N];
-  CT w[N];
-  ft_load_w(tw, 1.0, w);
+  CT* sZ2 = sZ1 + P * N * CPB * KS;           // [c' < P][b' < P] rows of ZS: [ch][slot], one pad
+  __shared__ CT sw[N];                        // w[m] = e^{+2 pi i m / N}, read by broadcast (passes A, B)
   if (tid < N) sw[tid] = CT{(R)tw[2 * tid], (R)tw[2 * tid + 1]};
   CT acc[NPT];
 #pragma unroll
   for (int i = 0; i < NPT; i++) acc[i] = CT{(R)0, (R)0};
   const int64_t fstride = (int64_t)N * N * nt * 8;
-  for (int j0 = 0; j0 < P; j0 += FTC_JS) {
+  for (int j0 = 0; j0 < P; j0 += JS) {
     __syncthreads();  // sw ready; the previous slab's sZ2 reads done
     // pass A, along kc, to c = P + c': task (kb, slot, ch), children fastest (one row per frequency)
     for (int e = tid; e < N * KS * CPB; e += FT_NT) {
@@ -2039,7 +2048,7 @@ __global__ void __launch_bounds__(FT_NT, 1)
         up[k] = CT{a.x + b.x, a.y + b.y};
         um[k] = CT{a.x - b.x, a.y - b.y};
       }
-      ftc_idft_upper<P>(up, um, w, [&](int cc, CT v) { sZ1[((cc * N + kb) * CPB + ch) * KS + sl] = v; });
+      ftc_idft_upper<P>(up, um, sw, [&](int cc, CT v) { sZ1[((cc * N + kb) * CPB + ch) * KS + sl] = v; });
     }
     __syncthreads();
     // pass B, along kb, to b = P + b': task (c', ch, slot)
@@ -2053,7 +2062,7 @@ __global__ void __launch_bounds__(FT_NT, 1)
         up[k] = CT{a.x + b.x, a.y + b.y};
         um[k] = CT{a.x - b.x, a.y - b.y};
       }
-      ftc_idft_upper<P>(up, um, w, [&](int bb, CT v) { sZ2[((cc * P + bb) * CPB + ch) * KS + sl] = v; });
+      ftc_idft_upper<P>(up, um, sw, [&](int bb, CT v) { sZ2[(cc * P + bb) * ZS + ch * KS + sl] = v; });
     }
     __syncthreads();
     // pass C, this slab's terms of the sum along ka at each point: (Z[j] + (-1)^a Z[j + P]) w^{j a}
@@ -2063,10 +2072,10 @@ __global__ void __launch_bounds__(FT_NT, 1)
       if (e < CPB * nsurf) {
         const int ch = e / nsurf, k = e - ch * nsurf, g = map_dn[k];
         const int a = g % N, b = g / N % N - P, c = g / (N * N) - P;
-        const CT* z = sZ2 + ((c * P + b) * CPB + ch) * KS;
+        const CT* z = sZ2 + (c * P + b) * ZS + ch * KS;
         const R sgn = (a & 1) ? (R)-1 : (R)1;
 #pragma unroll
-        for (int q = 0; q < FTC_JS; q++) {
+        for (int q = 0; q < JS; q++) {
           const int jj = j0 + q;
           if (jj >= P) break;
           const CT v{z[2 * q].x + sgn * z[2 * q + 1].x, z[2 * q].y + sgn * z[2 * q + 1].y};
