@@ -287,7 +287,7 @@ def roofline(r, peaks, src):
                  + nt * spec + nt * 8 * nsurf * 4 * 2)  # backward: products in, dn read-modify-write
     m2l_ms = st["M2L_fft"] + st["M2L_hadamard"] + st["M2L_ifft"]
     m2l = {"bound": "hbm", "achieved": m2l_bytes / (m2l_ms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-           "kernel": "k_m2l_fwd + k_hadamard_dt/k_hadamard_rt (tensor cores) + k_m2l_bwd (M2L)", "algorithmic_bytes": m2l_bytes,
+           "kernel": "k_m2l_fwd_r + k_hadamard_dt/k_hadamard_rt (tensor cores) + k_m2l_bwd_r (M2L)", "algorithmic_bytes": m2l_bytes,
            "ms": m2l_ms, "ms_transforms": st["M2L_fft"] + st["M2L_ifft"], "ms_hadamard": st["M2L_hadamard"],
            "peak_source": src}
     m2l["frac"] = m2l["achieved"] / m2l["peak"]

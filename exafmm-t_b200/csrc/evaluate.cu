@@ -6,9 +6,9 @@
 //                                                        (pinv factors), scaled scatter (0.5^l)
 //   M2M   fmm_scale_invariant.h:233-253 / fmm.h:221-241  row gather + library GEMM per level, K = 8 nsurf
 //   P2L   fmm_base.h:127-154                             k_p2l
-//   M2L   fmm_scale_invariant.h:407-440, 560-646;        real kernels: k_m2l_fwd + k_hadamard_dt/_rt (opt-in:
-//         fmm.h:395-446, 631-788                         k_hadamard_dc on tcgen05) + k_m2l_bwd (FP64:
-//                                                        k_hadamard); complex kernel (p <= 12): k_m2l_fwd_c
+//   M2L   fmm_scale_invariant.h:407-440, 560-646;        real kernels: k_m2l_fwd_r + k_hadamard_dt/_rt (opt-in:
+//         fmm.h:395-446, 631-788                         k_hadamard_dc on tcgen05) + k_m2l_bwd_r (FP64:
+//                                                        k_hadamard, k_m2l_bwd); complex kernel (p <= 12): k_m2l_fwd_c
 //                                                        + Hadamard + k_m2l_bwd_c; real p > 10 or p > 12:
 //                                                        k_m2l_grid_up + cuFFT + k_transpose + Hadamard +
 //                                                        k_transpose + cuFFT + k_m2l_gather_dn
@@ -1637,10 +1637,11 @@ __global__ void __launch_bounds__(HADC_NT, 2)
 // FFTW plans (fmm_scale_invariant.h:560-646).  Because only a p^3 corner of each input is non-zero and
 // only a p^3 corner of each output is used, both are computed as three passes of direct sums, one axis
 // at a time, in shared memory: no grid is materialised, and each spectrum value is written once by
-// k_m2l_fwd and read once by k_m2l_bwd, in the Hadamard product's [frequency][node][child] layout.
-// A CTA handles FT_CPB(R) children of one node: their spectrum values of one frequency are contiguous.
-// The expansion order P is a template parameter (2 <= P <= FT_PMAX), so every loop unrolls and each
-// DFT factor w^(jk mod n1) is a register chosen at compile time.
+// the forward transform (k_m2l_fwd_r, below) and read once by the backward one (k_m2l_bwd_r below; FP64:
+// k_m2l_bwd here), in the Hadamard product's [frequency][node][child] layout.  A CTA handles FtCpb(R)
+// children of one node: their spectrum values of one frequency are contiguous.  The expansion order P
+// is a template parameter (2 <= P <= FT_PMAX), so every loop unrolls; k_m2l_bwd keeps each DFT factor
+// w^(jk mod n1) in a register chosen at compile time.
 constexpr int FT_NT = 256;
 constexpr int FT_PMAX = 10;
 template <class R> struct FtCpb;
@@ -1668,7 +1669,7 @@ void ft_dispatch(int p, F&& fn) {
 }
 
 template <class R>
-size_t ft_fwd_smem(int p) {
+size_t ft_fwd_smem(int p) {  // k_m2l_bwd's shared memory: [CPB][p][n1][H] + [CPB][p][p][H] complex values
   const int n1 = 2 * p, h = p + 1, cpb = FtCpb<R>::v;
   return sizeof(typename C2<R>::type) * ((size_t)cpb * p * p * h + (size_t)cpb * p * n1 * h);
 }
@@ -1686,87 +1687,6 @@ __device__ __forceinline__ void ft_load_w(const double* __restrict__ tw, double 
   for (int m = 0; m < N; m++) {
     w[m].x = (decltype(w[m].x))tw[2 * m];
     w[m].y = (decltype(w[m].x))(sign * tw[2 * m + 1]);
-  }
-}
-
-// spec[(f*ns + s)*8 + child] = forward DFT of child `child` of source node src[s]
-template <class R, int P>
-__global__ void __launch_bounds__(FT_NT, FtMinB<R>::v)
-    k_m2l_fwd(const int* __restrict__ src, int ns, const int* __restrict__ child0, const R* __restrict__ up, int nsurf,
-              const int* __restrict__ map_up, const double* __restrict__ tw, typename C2<R>::type* __restrict__ spec) {
-  using CT = typename C2<R>::type;
-  constexpr int CPB = FtCpb<R>::v, N = 2 * P, H = P + 1, NC = N * H;
-  const int s = blockIdx.x, ch0 = blockIdx.y * CPB, tid = threadIdx.x;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  CT* sA = reinterpret_cast<CT*>(smem_raw);  // [CPB][c < P][b < P][ka < H]
-  CT* sB = sA + CPB * P * P * H;             // [CPB][c < P][kb < N][ka < H]
-  R* sx = reinterpret_cast<R*>(sB);          // [CPB][c][b][a < P], dead before sB is written
-  CT w[N];
-  ft_load_w(tw, -1.0, w);
-  for (int e = tid; e < CPB * P * P * P; e += FT_NT) sx[e] = (R)0;
-  __syncthreads();
-  const int64_t node0 = (int64_t)child0[src[s]] + ch0;
-  for (int e = tid; e < CPB * nsurf; e += FT_NT) {
-    const int ch = e / nsurf, k = e - ch * nsurf, g = map_up[k];
-    const int a = g % N, b = (g / N) % N, c = g / (N * N);
-    sx[((ch * P + c) * P + b) * P + a] = up[(node0 + ch) * nsurf + k];
-  }
-  __syncthreads();
-  // pass 1, along a (real input), one row (ch, c, b) per task: sA[row][ka] = sum_a x[row][a] w^{ka a}
-  for (int row = tid; row < CPB * P * P; row += FT_NT) {
-    R x[P];
-#pragma unroll
-    for (int a = 0; a < P; a++) x[a] = sx[row * P + a];
-#pragma unroll
-    for (int ka = 0; ka < H; ka++) {
-      R re = 0, im = 0;
-#pragma unroll
-      for (int a = 0; a < P; a++) {
-        re += x[a] * w[(ka * a) % N].x;
-        im += x[a] * w[(ka * a) % N].y;
-      }
-      sA[row * H + ka] = CT{re, im};
-    }
-  }
-  __syncthreads();
-  // pass 2, along b, one column (ch, c, ka) per task: sB[(cc N + kb) H + ka] = sum_b sA[(cc P + b) H + ka] w^{kb b}.
-  // Even and odd b summed apart: w^{(kb + P) b} = (-1)^b w^{kb b} (N = 2P), so outputs kb and kb + P are
-  // even + odd and even - odd.
-  for (int e = tid; e < CPB * P * H; e += FT_NT) {
-    const int ka = e % H, cc = e / H;
-    CT v[P];
-#pragma unroll
-    for (int b = 0; b < P; b++) v[b] = sA[(cc * P + b) * H + ka];
-#pragma unroll
-    for (int kb = 0; kb < P; kb++) {
-      CT ev = v[0], od = ft_mul(v[1], w[kb % N]);
-#pragma unroll
-      for (int b = 2; b < P; b += 2) vfma(ev, v[b], w[(kb * b) % N]);
-#pragma unroll
-      for (int b = 3; b < P; b += 2) vfma(od, v[b], w[(kb * b) % N]);
-      sB[(cc * N + kb) * H + ka] = CT{ev.x + od.x, ev.y + od.y};
-      sB[(cc * N + kb + P) * H + ka] = CT{ev.x - od.x, ev.y - od.y};
-    }
-  }
-  __syncthreads();
-  // pass 3, along c, one column (ch, kb, ka) per task: spec[f = (kc N + kb) H + ka][s][ch0 + ch]
-  for (int e = tid; e < NC * CPB; e += FT_NT) {
-    const int ch = e % CPB, col = e / CPB;
-    CT v[P];
-#pragma unroll
-    for (int c = 0; c < P; c++) v[c] = sB[(ch * P + c) * NC + col];
-    CT* o = spec + ((int64_t)col * ns + s) * 8 + ch0 + ch;
-    const int64_t fstride = (int64_t)NC * ns * 8;
-#pragma unroll
-    for (int kc = 0; kc < P; kc++) {  // outputs kc and kc + P from the even and odd c sums, as in pass 2
-      CT ev = v[0], od = ft_mul(v[1], w[kc % N]);
-#pragma unroll
-      for (int c = 2; c < P; c += 2) vfma(ev, v[c], w[(kc * c) % N]);
-#pragma unroll
-      for (int c = 3; c < P; c += 2) vfma(od, v[c], w[(kc * c) % N]);
-      o[kc * fstride] = CT{ev.x + od.x, ev.y + od.y};
-      o[(kc + P) * fstride] = CT{ev.x - od.x, ev.y - od.y};
-    }
   }
 }
 
@@ -1877,8 +1797,8 @@ void ftc_dispatch(int p, F&& fn) {
 }
 // y[k] for k < 2P from x[0..P): y[k] = sum_m x[m] w^{k m}, w[j] = e^{sign 2 pi i j / 2P}; outputs k and
 // k + P are even + odd and even - odd (w^{(k + P) m} = (-1)^m w^{k m}); out(k, value) stores one output
-template <int P, class CT, class Out>
-__device__ __forceinline__ void ftc_dft_p(const CT (&x)[P], const CT (&w)[2 * P], Out&& out) {
+template <int P, class CT, class WT, class Out>
+__device__ __forceinline__ void ftc_dft_p(const CT (&x)[P], const WT& w, Out&& out) {
   constexpr int N = 2 * P;
 #pragma unroll
   for (int k = 0; k < P; k++) {
@@ -2093,6 +2013,186 @@ __global__ void __launch_bounds__(FT_NT, FtcMinB<R>::v)
       CT* d = dn + node0 * nsurf + e;  // child ch0 + e / nsurf, point e % nsurf
       *d = CT{d->x + sc * acc[i].x, d->y + sc * acc[i].y};
     }
+  }
+}
+
+// ---------------------------------------------------------------- slabbed M2L transforms of the real kernels
+// The real transforms (half spectrum along the first axis, H = p + 1 frequencies ka) computed as the
+// complex ones are: CPB children per CTA (one spectrum row of a frequency read or written by consecutive
+// lanes), the first-axis frequencies in slabs of FTR_KS, so that a CTA needs ~37 KB of shared memory
+// (p = 8) instead of 110 KB and three or more CTAs share an SM; DFT factors are read from shared memory
+// (the same factor in every lane: broadcast).  The backward transform keeps each check point's running
+// sum along the last axis in registers across the slabs.
+#ifndef XFMM_FTR_KS
+#define XFMM_FTR_KS 3
+#endif
+#ifndef XFMM_FTR_MINB_F
+#define XFMM_FTR_MINB_F 4
+#endif
+constexpr int FTR_KS = XFMM_FTR_KS;
+template <class R> struct FtrMinB;
+template <> struct FtrMinB<float> { static constexpr int v = XFMM_FTR_MINB_F; };
+template <> struct FtrMinB<double> { static constexpr int v = 1; };
+template <class R>
+size_t ftr_fwd_smem(int p) {  // [p][p][CPB][KS] + [p][n1][CPB][KS] complex values
+  return sizeof(typename C2<R>::type) * (size_t)p * 3 * p * FtCpb<R>::v * FTR_KS;
+}
+template <class R>
+size_t ftr_bwd_smem(int p) {  // [p][n1][CPB][KS] + [p][p] rows of CPB KS + 1 complex values
+  const size_t zs = (size_t)FtCpb<R>::v * FTR_KS;
+  return sizeof(typename C2<R>::type) * ((size_t)p * 2 * p * zs + (size_t)p * p * (zs + 1));
+}
+
+// spec[(f*ns + s)*8 + ch0 + ch] = forward real-to-half-complex DFT of the children ch0 .. ch0 + CPB - 1 of
+// source node src[s], f = (kc n1 + kb) H + ka
+template <class R, int P>
+__global__ void __launch_bounds__(FT_NT, FtrMinB<R>::v)
+    k_m2l_fwd_r(const int* __restrict__ src, int ns, const int* __restrict__ child0, const R* __restrict__ up,
+                int nsurf, const int* __restrict__ conv2surf, const double* __restrict__ tw,
+                typename C2<R>::type* __restrict__ spec) {
+  using CT = typename C2<R>::type;
+  constexpr int N = 2 * P, H = P + 1, CPB = FtCpb<R>::v, KS = FTR_KS;
+  const int s = blockIdx.x, ch0 = blockIdx.y * CPB, tid = threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* sA = reinterpret_cast<CT*>(smem_raw);  // [c < P][b < P][ch][slot < KS]
+  CT* sB = sA + P * P * CPB * KS;            // [c < P][kb < N][ch][slot]
+  __shared__ int sidx[P * P * P];            // grid corner [c][b][a] -> surface index or -1
+  __shared__ CT sw[N];                       // w[m] = e^{-2 pi i m / N}
+  if (tid < N) sw[tid] = CT{(R)tw[2 * tid], (R)(-tw[2 * tid + 1])};
+  for (int e = tid; e < P * P * P; e += FT_NT) {
+    const int a = e % P, b = (e / P) % P, c = e / (P * P);
+    sidx[e] = conv2surf[(c * N + b) * N + a];
+  }
+  const int64_t node0 = (int64_t)child0[src[s]] + ch0;
+  const int64_t fstride = (int64_t)N * H * ns * 8;  // kc -> kc + 1
+  for (int k0 = 0; k0 < H; k0 += KS) {
+    __syncthreads();  // sidx and sw ready; the previous slab's reads done
+    // pass 1, along a (real input): task (c, b, ch), slot sl = ka - k0
+    for (int e = tid; e < P * P * CPB; e += FT_NT) {
+      const int ch = e % CPB, cb = e / CPB;
+      const R* u = up + (node0 + ch) * nsurf;
+      R x[P];
+#pragma unroll
+      for (int a = 0; a < P; a++) {
+        const int k = sidx[cb * P + a];
+        x[a] = k >= 0 ? __ldg(u + k) : (R)0;
+      }
+#pragma unroll
+      for (int sl = 0; sl < KS; sl++) {
+        const int ka = k0 + sl;
+        if (ka >= H) break;
+        R re = x[0], im = 0;
+#pragma unroll
+        for (int a = 1; a < P; a++) {
+          const CT ww = sw[(ka * a) % N];
+          re += x[a] * ww.x;
+          im += x[a] * ww.y;
+        }
+        sA[(cb * CPB + ch) * KS + sl] = CT{re, im};
+      }
+    }
+    __syncthreads();
+    // pass 2, along b: task (c, ch, slot)
+    for (int e = tid; e < P * CPB * KS; e += FT_NT) {
+      const int sl = e % KS, ch = (e / KS) % CPB, c = e / (KS * CPB);
+      if (k0 + sl >= H) continue;
+      CT x[P];
+#pragma unroll
+      for (int b = 0; b < P; b++) x[b] = sA[((c * P + b) * CPB + ch) * KS + sl];
+      ftc_dft_p<P>(x, sw, [&](int kb, CT v) { sB[((c * N + kb) * CPB + ch) * KS + sl] = v; });
+    }
+    __syncthreads();
+    // pass 3, along c: task (kb, slot, ch), children fastest
+    for (int e = tid; e < N * KS * CPB; e += FT_NT) {
+      const int ch = e % CPB, sl = (e / CPB) % KS, kb = e / (CPB * KS);
+      const int ka = k0 + sl;
+      if (ka >= H) continue;
+      CT x[P];
+#pragma unroll
+      for (int c = 0; c < P; c++) x[c] = sB[((c * N + kb) * CPB + ch) * KS + sl];
+      CT* o = spec + ((int64_t)(kb * H + ka) * ns + s) * 8 + ch0 + ch;
+      ftc_dft_p<P>(x, sw, [&](int kc, CT v) { o[kc * fstride] = v; });
+    }
+  }
+}
+
+// dn[child ch0 + ch of target trg[t]][k] += scale[t] * backward half-complex-to-real DFT of spec[.][t][child]
+// at map_dn[k] (weight 2 on the half spectrum's interior frequencies 0 < ka < N / 2)
+template <class R, int P>
+__global__ void __launch_bounds__(FT_NT, FtrMinB<R>::v)
+    k_m2l_bwd_r(const int* __restrict__ trg, int nt, const int* __restrict__ child0,
+                const typename C2<R>::type* __restrict__ spec, int nsurf, const int* __restrict__ map_dn,
+                const double* __restrict__ tw, const R* __restrict__ scale, R* __restrict__ dn) {
+  using CT = typename C2<R>::type;
+  constexpr int N = 2 * P, H = P + 1, CPB = FtCpb<R>::v, KS = FTR_KS, ZS = CPB * KS + 1;
+  constexpr int NPT = (CPB * (6 * (P - 1) * (P - 1) + 2) + FT_NT - 1) / FT_NT;  // points per thread
+  const int t = blockIdx.x, ch0 = blockIdx.y * CPB, tid = threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* sZ1 = reinterpret_cast<CT*>(smem_raw);  // [c' < P][kb < N][ch][slot < KS]
+  CT* sZ2 = sZ1 + P * N * CPB * KS;           // [c' < P][b' < P] rows of ZS: [ch][slot], one pad
+  __shared__ CT sw[N];                        // w[m] = e^{+2 pi i m / N}
+  if (tid < N) sw[tid] = CT{(R)tw[2 * tid], (R)tw[2 * tid + 1]};
+  R acc[NPT];
+#pragma unroll
+  for (int i = 0; i < NPT; i++) acc[i] = 0;
+  const int64_t fstride = (int64_t)N * H * nt * 8;
+  for (int k0 = 0; k0 < H; k0 += KS) {
+    __syncthreads();  // sw ready; the previous slab's sZ2 reads done
+    // pass A, along kc, to c = P + c': task (kb, slot, ch), children fastest
+    for (int e = tid; e < N * KS * CPB; e += FT_NT) {
+      const int ch = e % CPB, sl = (e / CPB) % KS, kb = e / (CPB * KS);
+      const int ka = k0 + sl;
+      if (ka >= H) continue;
+      const CT* y = spec + ((int64_t)(kb * H + ka) * nt + t) * 8 + ch0 + ch;
+      CT up[P], um[P];
+#pragma unroll
+      for (int k = 0; k < P; k++) {
+        const CT a = y[k * fstride], b = y[(k + P) * fstride];
+        up[k] = CT{a.x + b.x, a.y + b.y};
+        um[k] = CT{a.x - b.x, a.y - b.y};
+      }
+      ftc_idft_upper<P>(up, um, sw, [&](int cc, CT v) { sZ1[((cc * N + kb) * CPB + ch) * KS + sl] = v; });
+    }
+    __syncthreads();
+    // pass B, along kb, to b = P + b': task (c', ch, slot)
+    for (int e = tid; e < P * CPB * KS; e += FT_NT) {
+      const int sl = e % KS, ch = (e / KS) % CPB, cc = e / (KS * CPB);
+      if (k0 + sl >= H) continue;
+      CT up[P], um[P];
+#pragma unroll
+      for (int k = 0; k < P; k++) {
+        const CT a = sZ1[((cc * N + k) * CPB + ch) * KS + sl], b = sZ1[((cc * N + k + P) * CPB + ch) * KS + sl];
+        up[k] = CT{a.x + b.x, a.y + b.y};
+        um[k] = CT{a.x - b.x, a.y - b.y};
+      }
+      ftc_idft_upper<P>(up, um, sw, [&](int bb, CT v) { sZ2[(cc * P + bb) * ZS + ch * KS + sl] = v; });
+    }
+    __syncthreads();
+    // pass C, this slab's terms along ka at each point: wgt Re(Z[ka] w^{ka a})
+#pragma unroll
+    for (int i = 0; i < NPT; i++) {
+      const int e = tid + i * FT_NT;
+      if (e < CPB * nsurf) {
+        const int ch = e / nsurf, k = e - ch * nsurf, g = map_dn[k];
+        const int a = g % N, b = g / N % N - P, c = g / (N * N) - P;
+        const CT* z = sZ2 + (c * P + b) * ZS + ch * KS;
+#pragma unroll
+        for (int sl = 0; sl < KS; sl++) {
+          const int ka = k0 + sl;
+          if (ka >= H) break;
+          const CT ww = sw[(ka * a) % N];
+          const R wgt = (ka == 0 || 2 * ka == N) ? (R)1 : (R)2;
+          acc[i] += wgt * (z[sl].x * ww.x - z[sl].y * ww.y);
+        }
+      }
+    }
+  }
+  const int64_t node0 = (int64_t)child0[trg[t]] + ch0;
+  const R sc = scale[t];
+#pragma unroll
+  for (int i = 0; i < NPT; i++) {
+    const int e = tid + i * FT_NT;
+    if (e < CPB * nsurf) dn[node0 * nsurf + e] += sc * acc[i];  // child ch0 + e / nsurf, point e % nsurf
   }
 }
 
@@ -2336,7 +2436,7 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   const size_t rsz = f.mixed() ? 4 : 8;  // real scalar size
   {
     constexpr size_t kMaxSmem = 227 * 1024;
-    const size_t fw = f.mixed() ? ft_fwd_smem<float>(f.p) : ft_fwd_smem<double>(f.p);
+    const size_t fw = f.mixed() ? ftr_fwd_smem<float>(f.p) : ftr_fwd_smem<double>(f.p);
     const size_t bw = f.mixed() ? ft_bwd_smem<float>(f.p) : ft_bwd_smem<double>(f.p);
     const size_t cw = std::max(f.mixed() ? ftc_fwd_smem<float>(f.p) : ftc_fwd_smem<double>(f.p),
                                f.mixed() ? ftc_bwd_smem<float>(f.p) : ftc_bwd_smem<double>(f.p));
@@ -2589,13 +2689,13 @@ struct Engine {
         if (ws.fused) {
           ft_dispatch(f.p, [&](auto pc) {
             constexpr int PP = decltype(pc)::value;
-            const size_t smem = ft_fwd_smem<R>(PP);
+            const size_t smem = ftr_fwd_smem<R>(PP);
             if (ws.ft_fwd_smem < smem) {
-              XCUDA(cudaFuncSetAttribute(k_m2l_fwd<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+              XCUDA(cudaFuncSetAttribute(k_m2l_fwd_r<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
               ws.ft_fwd_smem = smem;
             }
-            k_m2l_fwd<R, PP><<<dim3(ns, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
-                src, ns, t.child0.p, (const R*)ws.up.p, n, f.map_up.p, f.dft_tw.p, (CT*)ws.specB.p);
+            k_m2l_fwd_r<R, PP><<<dim3(ns, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
+                src, ns, t.child0.p, (const R*)ws.up.p, n, f.conv_to_surf_up.p, f.dft_tw.p, (CT*)ws.specB.p);
           });
           XLAUNCH();
           ws.launches++;
@@ -2691,6 +2791,18 @@ struct Engine {
         if (ws.fused) {
           ft_dispatch(f.p, [&](auto pc) {
             constexpr int PP = decltype(pc)::value;
+          if constexpr (sizeof(R) == 4) {  // FP64: the unslabbed form (measured faster at 1 CTA per SM)
+            const size_t smem = ftr_bwd_smem<R>(PP);
+            if (ws.ft_bwd_smem < smem) {
+              XCUDA(cudaFuncSetAttribute(k_m2l_bwd_r<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+              ws.ft_bwd_smem = smem;
+            }
+            k_m2l_bwd_r<R, PP><<<dim3(nt, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
+                trg, nt, t.child0.p, (const CT*)ws.specA.p, n, f.map_dn.p, f.dft_tw.p,
+                m2l_scale_of<R>(t) + t.m2l_trg_off[g], (R*)ws.dn.p);
+            return;
+          }
+          {
             const size_t smem = ft_bwd_smem<R>(PP);
             if (ws.ft_bwd_smem < smem) {
               XCUDA(cudaFuncSetAttribute(k_m2l_bwd<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -2699,6 +2811,7 @@ struct Engine {
             k_m2l_bwd<R, PP><<<dim3(nt, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
                 trg, nt, t.child0.p, (const CT*)ws.specA.p, n, f.map_dn.p, f.dft_tw.p,
                 m2l_scale_of<R>(t) + t.m2l_trg_off[g], (R*)ws.dn.p);
+          }
           });
           XLAUNCH();
           ws.launches++;
