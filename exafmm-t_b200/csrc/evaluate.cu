@@ -1647,8 +1647,7 @@ constexpr int FT_PMAX = 10;
 template <class R> struct FtCpb;
 template <> struct FtCpb<float> { static constexpr int v = 8; };   // 64-byte chunks of float2
 template <> struct FtCpb<double> { static constexpr int v = 4; };  // 64-byte chunks of double2
-template <class R> struct FtMinB;
-template <> struct FtMinB<float> { static constexpr int v = 2; };
+template <class R> struct FtMinB;  // k_m2l_bwd (FP64 only)
 template <> struct FtMinB<double> { static constexpr int v = 1; };
 
 // calls fn(std::integral_constant<int, p>) for 2 <= p <= FT_PMAX
@@ -2800,9 +2799,7 @@ struct Engine {
             k_m2l_bwd_r<R, PP><<<dim3(nt, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
                 trg, nt, t.child0.p, (const CT*)ws.specA.p, n, f.map_dn.p, f.dft_tw.p,
                 m2l_scale_of<R>(t) + t.m2l_trg_off[g], (R*)ws.dn.p);
-            return;
-          }
-          {
+          } else {
             const size_t smem = ft_bwd_smem<R>(PP);
             if (ws.ft_bwd_smem < smem) {
               XCUDA(cudaFuncSetAttribute(k_m2l_bwd<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
