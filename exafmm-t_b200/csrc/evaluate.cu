@@ -2029,9 +2029,15 @@ __global__ void __launch_bounds__(FT_NT, FtcMinB<R>::v)
 #define XFMM_FTR_MINB_F 4
 #endif
 constexpr int FTR_KS = XFMM_FTR_KS;
+#ifndef XFMM_FTR_BWD_MINB_HI
+#define XFMM_FTR_BWD_MINB_HI 3  // backward transform, p >= 9 (more per-point sums per thread; measured at p = 10)
+#endif
 template <class R> struct FtrMinB;
 template <> struct FtrMinB<float> { static constexpr int v = XFMM_FTR_MINB_F; };
 template <> struct FtrMinB<double> { static constexpr int v = 1; };
+template <class R, int P> struct FtrBwdMinB {
+  static constexpr int v = (sizeof(R) == 4 && P >= 9) ? XFMM_FTR_BWD_MINB_HI : FtrMinB<R>::v;
+};
 template <class R>
 size_t ftr_fwd_smem(int p) {  // [p][p][CPB][KS] + [p][n1][CPB][KS] complex values
   return sizeof(typename C2<R>::type) * (size_t)p * 3 * p * FtCpb<R>::v * FTR_KS;
@@ -2118,7 +2124,7 @@ __global__ void __launch_bounds__(FT_NT, FtrMinB<R>::v)
 // dn[child ch0 + ch of target trg[t]][k] += scale[t] * backward half-complex-to-real DFT of spec[.][t][child]
 // at map_dn[k] (weight 2 on the half spectrum's interior frequencies 0 < ka < N / 2)
 template <class R, int P>
-__global__ void __launch_bounds__(FT_NT, FtrMinB<R>::v)
+__global__ void __launch_bounds__(FT_NT, (FtrBwdMinB<R, P>::v))
     k_m2l_bwd_r(const int* __restrict__ trg, int nt, const int* __restrict__ child0,
                 const typename C2<R>::type* __restrict__ spec, int nsurf, const int* __restrict__ map_dn,
                 const double* __restrict__ tw, const R* __restrict__ scale, R* __restrict__ dn) {
