@@ -178,3 +178,30 @@ def test_hadamard_tcgen05_form(monkeypatch):
         outs.append(out)
     pe, ge = orc.rel_l2(outs[1], outs[0])
     assert pe < 5e-7 and ge < 5e-7, (pe, ge)
+
+
+# Orders beyond the fixtures: the slabbed real transforms at p = 9 (odd order: a partial last slab) and
+# p = 10 (the other occupancy setting), and the complex transforms at p = 9 and p = 12, against FP64
+# direct sums; the mixed path also against the FP64 path on the same tree.
+@pytest.mark.parametrize("kernel,p,wk", [("laplace", 9, 0.0), ("laplace", 10, 0.0),
+                                         ("helmholtz", 9, 20.0), ("helmholtz", 12, 20.0)])
+def test_high_orders_against_direct_sums(kernel, p, wk):
+    rng = np.random.default_rng(11)
+    n = 20000
+    x = rng.random((n, 3))
+    q = rng.uniform(-1, 1, n)
+    if kernel == "helmholtz":
+        q = q + 1j * rng.uniform(-1, 1, n)
+    m = _mod(kernel)
+    outs = {}
+    for prec in ("fp64", "mixed"):
+        fmm = (m.LaplaceFmm(p, 64, precision=prec) if kernel == "laplace"
+               else m.HelmholtzFmm(p, 64, wk, precision=prec))
+        tree = m.setup(m.init_sources(x, q), m.init_targets(x), fmm)
+        outs[prec] = m.evaluate(tree, fmm)
+    s = rng.choice(n, 300, replace=False)
+    ex = orc.direct(kernel, x, q, x[s], wk)
+    pe, ge = orc.rel_l2(outs["fp64"][s], ex)
+    assert pe < 1e-4 and ge < 1e-3, (pe, ge)        # bounded by the FMM's own truncation error
+    pm, gm = orc.rel_l2(outs["mixed"], outs["fp64"])
+    assert pm < 5e-6 and gm < 5e-6, (pm, gm)        # mixed precision against FP64 on the same tree
