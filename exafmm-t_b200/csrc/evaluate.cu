@@ -1834,6 +1834,10 @@ template <> struct FtcCpb<double> { static constexpr int v = 4; };
 #define XFMM_FTC_JS 3
 #endif
 constexpr int FTC_JS = XFMM_FTC_JS;  // first-axis base frequencies j per slab: outputs ka = j and j + p
+#ifndef XFMM_FTC_FWD_MINB
+#define XFMM_FTC_FWD_MINB 1  // FP32: resident CTAs per SM the forward transform's registers are set for
+#endif
+template <class R> struct FtcFwdMinB { static constexpr int v = sizeof(R) == 4 ? XFMM_FTC_FWD_MINB : 1; };
 template <class R>
 size_t ftc_fwd_smem(int p) {  // per child and slab: [p][p][2 JS] + [p][n1][2 JS] complex values
   return sizeof(typename C2<R>::type) * FtcCpb<R>::v * (size_t)p * (p + 2 * p) * 2 * FTC_JS;
@@ -1855,7 +1859,7 @@ size_t ftc_bwd_smem(int p) {
 // partners j + p); per slab the three passes run on the slab's columns only, and the grid input is read
 // through the grid -> surface map (values outside the surface are zero) from the L1-resident rows of up.
 template <class R, int P>
-__global__ void __launch_bounds__(FT_NT, 1)
+__global__ void __launch_bounds__(FT_NT, FtcFwdMinB<R>::v)
     k_m2l_fwd_c(const int* __restrict__ src, int ns, const int* __restrict__ child0,
                 const typename C2<R>::type* __restrict__ up, int nsurf, const int* __restrict__ conv2surf,
                 const double* __restrict__ tw, typename C2<R>::type* __restrict__ spec) {
@@ -1866,9 +1870,7 @@ __global__ void __launch_bounds__(FT_NT, 1)
   CT* sA = reinterpret_cast<CT*>(smem_raw);  // [c < P][b < P][ch][slot < KS]
   CT* sB = sA + P * P * CPB * KS;            // [c < P][kb < N][ch][slot]
   __shared__ int sidx[P * P * P];            // grid corner [c][b][a] -> surface index or -1
-  __shared__ CT sw[N];                       // w[m] for run-time m (pass 1: the same m in every lane)
-  CT w[N];
-  ft_load_w(tw, -1.0, w);
+  __shared__ CT sw[N];                       // w[m] = e^{-2 pi i m / N}: the same factor in every lane
   if (tid < N) sw[tid] = CT{(R)tw[2 * tid], (R)(-tw[2 * tid + 1])};
   for (int e = tid; e < P * P * P; e += FT_NT) {
     const int a = e % P, b = (e / P) % P, c = e / (P * P);
@@ -1906,7 +1908,7 @@ __global__ void __launch_bounds__(FT_NT, 1)
       CT x[P];
 #pragma unroll
       for (int b = 0; b < P; b++) x[b] = sA[((c * P + b) * CPB + ch) * KS + sl];
-      ftc_dft_p<P>(x, w, [&](int kb, CT v) { sB[((c * N + kb) * CPB + ch) * KS + sl] = v; });
+      ftc_dft_p<P>(x, sw, [&](int kb, CT v) { sB[((c * N + kb) * CPB + ch) * KS + sl] = v; });
     }
     __syncthreads();
     // pass 3, along c: task (kb, slot, ch), children fastest: the CPB children of one frequency are
@@ -1920,7 +1922,7 @@ __global__ void __launch_bounds__(FT_NT, 1)
 #pragma unroll
       for (int c = 0; c < P; c++) x[c] = sB[((c * N + kb) * CPB + ch) * KS + sl];
       CT* o = spec + ((int64_t)(kb * N + ka) * ns + s) * 8 + ch0 + ch;
-      ftc_dft_p<P>(x, w, [&](int kc, CT v) { o[kc * fstride] = v; });
+      ftc_dft_p<P>(x, sw, [&](int kc, CT v) { o[kc * fstride] = v; });
     }
   }
 }
