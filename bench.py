@@ -343,7 +343,7 @@ def run_batched(args):
     t0 = time.perf_counter()
     b = BatchedFmm(systems, lambda: L.LaplaceFmm(6, 64, precision="mixed"))
     setup_s = time.perf_counter() - t0
-    b.autotune()  # concurrent streams inside the graph: the count with the fastest replay
+    b.autotune()  # concurrent streams inside the graph, then the sparse Hadamard's tiles per CTA
 
     def timed(fn):
         for _ in range(args.warmup):
@@ -370,6 +370,8 @@ def run_batched(args):
             "per_problem_launches": {"value": ntot / (ms_each * 1e-3) / 1e6, "ms_per_step": ms_each},
             "graph_speedup": ms_each / ms_graph, "setup_s": setup_s,
             "graph_streams": b.nstreams, "autotune_ms_per_replay": {str(k): round(v, 3) for k, v in b.tuning.items()},
+            "sparse_hadamard_tiles_per_cta": b.tiles_per_cta,
+            "autotune_tiles_ms_per_replay": {str(k): round(v, 3) for k, v in b.tile_tuning.items()},
             "clocks": clk.summary()}
     print(json.dumps(line))
 

@@ -302,6 +302,15 @@ xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms14) {
   });
 }
 
+xfmm_status xfmm_set_tuning(xfmm_tree* tree, int option, int value) {
+  return guarded([&] {
+    XREQUIRE(tree, XFMM_ERR_ARG, "null argument");
+    XREQUIRE(option == XFMM_TUNE_SPARSE_HADAMARD_TILES_PER_CTA, XFMM_ERR_ARG, "unknown tuning option");
+    XREQUIRE(value >= 0 && value <= 64, XFMM_ERR_ARG, "sparse Hadamard tiles per CTA must be 0..64");
+    tree->t.hadr_tpc = value;
+  });
+}
+
 xfmm_status xfmm_gradient_p2p(int kernel, double k_re, double k_im, int precision, const double* src_xyz,
                               int64_t nsrc, const double* q, const double* trg_xyz, int64_t ntrg, double* out,
                               int on_device, void* stream) {

@@ -1164,7 +1164,7 @@ constexpr int HADR_RW = 64;             // pairs per round (4 row tiles of 16)
 #ifndef XFMM_HADR_TPC
 #define XFMM_HADR_TPC 4
 #endif
-constexpr int HADR_TPC = XFMM_HADR_TPC;  // tiles per CTA (one B fill per frequency for all of them)
+constexpr int HADR_TPC = XFMM_HADR_TPC;  // default tiles per CTA (one B fill per frequency for all of them)
 
 
 // Hadamard product, dense form on the tensor cores (FP32 accuracy from three TF32 products).
@@ -1250,7 +1250,7 @@ __device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, co
 __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 registers, a 16-byte spill)
     k_hadamard_rt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
                   const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
-                  const int* __restrict__ rows, int ntiles, int nsrc, int ntrg, int nfreq) {
+                  const int* __restrict__ rows, int ntiles, int tpc, int nsrc, int ntrg, int nfreq) {
   constexpr int NW = HADR_NT / 32;
   static_assert(HADR_RW == 64, "a round is 4 row tiles of 16 pairs");
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1258,7 +1258,7 @@ __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 
   const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   // tiles [tb, te) share this CTA's B fragments of frequency f
-  const int tb = blockIdx.x * HADR_TPC, te = min(ntiles, tb + HADR_TPC);
+  const int tb = blockIdx.x * tpc, te = min(ntiles, tb + tpc);
   float2* of = out + (int64_t)f * ntrg * 8;
   // every product of these tiles' targets at frequency f is added by this CTA: their rows start at zero
   for (int e = tid; e < (te - tb) * HADR_TT * 4; e += HADR_NT) {
@@ -2742,9 +2742,10 @@ struct Engine {
             XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
             ws.hadrt_attr = true;
           }
-          k_hadamard_rt<<<dim3((ntiles + HADR_TPC - 1) / HADR_TPC, nfreq), HADR_NT, HADT_SMEM, s>>>(
+          const int tpc = t.hadr_tpc > 0 ? t.hadr_tpc : HADR_TPC;
+          k_hadamard_rt<<<dim3((ntiles + tpc - 1) / tpc, nfreq), HADR_NT, HADT_SMEM, s>>>(
               T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
-              ws.hadr_ent.p, rows, ntiles, ns, nt, nfreq);
+              ws.hadr_ent.p, rows, ntiles, tpc, ns, nt, nfreq);
           XLAUNCH();
           ws.launches++;
         }

@@ -147,6 +147,7 @@ struct Tree {
   // persistent staging for host-side charges and results (no allocation per call)
   DBuf<double> stage_q, stage_out;
   DBuf<int> stage_flag;               // non-finite charges found by the device-side check
+  int hadr_tpc = 0;                   // sparse M2L Hadamard: tiles per CTA (0: the built-in default)
 };
 
 // Precomputed operators of one level (or the single scale-invariant level).

@@ -179,6 +179,12 @@ class Tree:
         self._h, self.fmm, self.nsrc, self.ntrg = h, fmm, nsrc, ntrg
         self._dump = None
 
+    TUNING = {"sparse_hadamard_tiles_per_cta": 1}  # include/xfmm.h XFMM_TUNE_*
+
+    def set_tuning(self, name, value):
+        """Tile option for later evaluates of this tree (no reference counterpart); 0 restores the default."""
+        _lib.check(_lib.lib().xfmm_set_tuning(self._h, self.TUNING[name], int(value)))
+
     def info(self):
         v = np.zeros(12, np.int64)
         _lib.check(_lib.lib().xfmm_tree_info(self._h, v.ctypes.data))

@@ -39,6 +39,7 @@ SIGNATURES = [
     ("xfmm_tree_info", i32, [vp, vp]),
     ("xfmm_tree_dump", i32, [vp] * 17),
     ("xfmm_stage_times", i32, [vp, vp, vp]),
+    ("xfmm_set_tuning", i32, [vp, i32, i32]),
     ("xfmm_gradient_p2p", i32, [i32, f64, f64, i32, vp, i64, vp, vp, i64, vp, i32, vp]),
     ("xfmm_verify", i32, [vp, vp, i32, vp, vp]),
     ("xfmm_gradient_p2p_noalloc", i32, [i32, f64, f64, i32, vp, i64, vp, vp, i64, vp, vp]),

@@ -15,7 +15,8 @@ first, to the stream with the fewest bodies so far) and joins them again, so the
 systems share the GPU instead of running one after another.  Every system owns its operators, tree,
 work buffers and library handles (cuBLAS with a fixed workspace), so nothing is shared between the
 streams.  ``autotune()`` captures the graph for each candidate stream count, times replays on the
-device and keeps the fastest.
+device and keeps the fastest; then, at that stream count, it does the same for each candidate tile
+shape of the sparse M2L Hadamard (target tiles per CTA, set on every tree through xfmm_set_tuning).
 """
 import ctypes
 
@@ -48,7 +49,9 @@ class BatchedFmm:
         self._side = []
         self.graph = None
         self.nstreams = 1
-        self.tuning = {}
+        self.tuning = {}        # stream count -> ms per replay
+        self.tiles_per_cta = 0  # sparse Hadamard tiles per CTA on every tree (0: the library default)
+        self.tile_tuning = {}   # tiles per CTA -> ms per replay, at the chosen stream count
 
     def _enqueue(self, stream_handle, order=None):
         L = _lib.lib()
@@ -105,25 +108,49 @@ class BatchedFmm:
         self.nstreams = int(nstreams)
         return g
 
-    def autotune(self, candidates=(1, 2, 4, 8, 16, 32), reps=3):
+    def _time_graph(self, g, reps):
+        self.replay()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        for _ in range(reps):
+            with torch.cuda.stream(self.stream):
+                g.replay()
+        e1.record(self.stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def set_tiles_per_cta(self, value):
+        """Sparse M2L Hadamard tiles per CTA on every tree (0: the library default); recapture after."""
+        for tree in self.trees:
+            tree.set_tuning("sparse_hadamard_tiles_per_cta", value)
+        self.tiles_per_cta = int(value)
+
+    def autotune(self, candidates=(1, 2, 4, 8, 16, 32), reps=3, tile_candidates=(1, 2, 4, 8)):
         """Capture the graph for each stream count in candidates, time `reps` replays of each on the
-        device (after one untimed replay) and keep the fastest graph.  self.tuning maps each stream
-        count to its milliseconds per replay."""
+        device (after one untimed replay) and keep the fastest graph; then, at that stream count, the
+        same for each sparse-Hadamard tiles-per-CTA value in tile_candidates.  self.tuning maps each
+        stream count, self.tile_tuning each tile value, to its milliseconds per replay."""
+        self._autotune_streams(candidates, reps)
+        if tile_candidates:
+            best_ms, best_tiles = None, self.tiles_per_cta
+            for tiles in tile_candidates:
+                self.set_tiles_per_cta(tiles)
+                g = self.capture(self.nstreams)
+                self.tile_tuning[int(tiles)] = self._time_graph(g, reps)
+                if best_ms is None or self.tile_tuning[int(tiles)] < best_ms:
+                    best_ms, best_tiles = self.tile_tuning[int(tiles)], int(tiles)
+            self.set_tiles_per_cta(best_tiles)
+            self.capture(self.nstreams)
+        return self.nstreams
+
+    def _autotune_streams(self, candidates, reps):
         best = None
         for ns in candidates:
             ns = max(1, min(int(ns), len(self.n)))
             if ns in self.tuning:
                 continue
             g = self.capture(ns)
-            self.replay()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(self.stream)
-            for _ in range(reps):
-                with torch.cuda.stream(self.stream):
-                    g.replay()
-            e1.record(self.stream)
-            e1.synchronize()
-            self.tuning[ns] = e0.elapsed_time(e1) / reps
+            self.tuning[ns] = self._time_graph(g, reps)
             if best is None or self.tuning[ns] < self.tuning[best[0]]:
                 best = (ns, g)
             else:

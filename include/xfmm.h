@@ -114,6 +114,18 @@ xfmm_status xfmm_tree_dump(const xfmm_tree* tree, double* geo, uint64_t* key, in
  * results are then incomplete). */
 xfmm_status xfmm_stage_times(xfmm_fmm* fmm, xfmm_tree* tree, double* ms14);
 
+/* Tuning options of a tree's evaluate (xfmm_set_tuning). */
+enum {
+  /* mixed path, sparse M2L Hadamard (k_hadamard_rt): target tiles of 512 covered by one CTA, which
+   * builds the frequency's operator fragments once for all of them; 1..64, 0 restores the default (4) */
+  XFMM_TUNE_SPARSE_HADAMARD_TILES_PER_CTA = 1
+};
+/* Sets a tuning option for the later evaluates of this tree; results change only within the mixed
+ * path's run-to-run rounding.  No counterpart in the reference, whose loops have no tile parameters;
+ * it lets a caller's autotuner (exafmm.batch.BatchedFmm.autotune) search tile shapes.  XFMM_ERR_ARG for
+ * an unknown option or a value out of range. */
+xfmm_status xfmm_set_tuning(xfmm_tree* tree, int option, int value);
+
 /* Direct near-field kernel over raw arrays: out (ntrg x 4) += potential and gradient
  * at trg from (src, q).  precision selects the FP64 or FP32 device kernel. */
 xfmm_status xfmm_gradient_p2p(int kernel, double k_re, double k_im, int precision, const double* src_xyz,

@@ -68,3 +68,10 @@ def test_argument_errors():
         assert "must match" in str(e)
     else:
         raise AssertionError
+
+
+def test_tuning_option_arguments_checked_without_a_gpu():
+    from exafmm import _lib
+    L = _lib.lib()
+    assert L.xfmm_set_tuning(None, 1, 4) == 1  # XFMM_ERR_ARG: no tree
+    assert b"null" in L.xfmm_last_error()

@@ -42,9 +42,10 @@ def test_graph_on_concurrent_streams_equals_one_by_one_fp64():
 def test_autotune_keeps_a_timed_stream_count():
     systems, b = _batch("fp64")
     seq = [o.clone() for o in b.evaluate_each()]
-    ns = b.autotune(candidates=(1, 2, 4), reps=2)
+    ns = b.autotune(candidates=(1, 2, 4), reps=2, tile_candidates=(1, 4))
     assert ns in (1, 2, 4) and set(b.tuning) == {1, 2, 4}
     assert b.tuning[ns] == min(b.tuning.values())
+    assert set(b.tile_tuning) == {1, 4} and b.tile_tuning[b.tiles_per_cta] == min(b.tile_tuning.values())
     rep = b.replay()
     torch.cuda.synchronize()
     for a, c in zip(seq, rep):

@@ -205,3 +205,22 @@ def test_high_orders_against_direct_sums(kernel, p, wk):
     assert pe < 1e-4 and ge < 1e-3, (pe, ge)        # bounded by the FMM's own truncation error
     pm, gm = orc.rel_l2(outs["mixed"], outs["fp64"])
     assert pm < 5e-6 and gm < 5e-6, (pm, gm)        # mixed precision against FP64 on the same tree
+
+
+def test_sparse_hadamard_tile_option():
+    """xfmm_set_tuning: the sparse Hadamard's tiles per CTA change the launch, not the result (beyond
+    the mixed path's run-to-run rounding); out-of-range values are rejected."""
+    import exafmm.laplace as L
+    from exafmm._lib import FmmError
+    rng = np.random.default_rng(3)
+    x = rng.random((60000, 3))
+    q = rng.uniform(-1, 1, 60000)
+    fmm = L.LaplaceFmm(8, 64, precision="mixed")
+    tree = L.setup(L.init_sources(x, q), L.init_targets(x), fmm)
+    base = L.evaluate(tree, fmm)
+    for tiles in (1, 3, 64, 0):
+        tree.set_tuning("sparse_hadamard_tiles_per_cta", tiles)
+        pe, ge = orc.rel_l2(L.evaluate(tree, fmm), base)
+        assert pe < 1e-6 and ge < 1e-6, (tiles, pe, ge)
+    with pytest.raises(FmmError):
+        tree.set_tuning("sparse_hadamard_tiles_per_cta", 65)
