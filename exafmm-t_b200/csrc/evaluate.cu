@@ -1158,6 +1158,10 @@ __global__ void __launch_bounds__(128 * HadKC<CT>::KC) k_hadamard(const CT* __re
 #define XFMM_HAD_DENSE_MIN 12
 #endif
 constexpr int HAD_DENSE_MIN = XFMM_HAD_DENSE_MIN;  // occupied positions that make a target dense
+#ifndef XFMM_HAD_DENSE_GROUP_MIN
+#define XFMM_HAD_DENSE_GROUP_MIN 256
+#endif
+constexpr int HAD_DENSE_GROUP_MIN = XFMM_HAD_DENSE_GROUP_MIN;  // dense targets a group needs for the dense form
 constexpr int HADR_NT = 256;            // threads per CTA
 constexpr int HADR_TT = 512;            // targets per tile
 constexpr int HADR_RW = 64;             // pairs per round (4 row tiles of 16)
@@ -2489,6 +2493,13 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
         int cnt = 0;
         for (int ipos = 0; ipos < 26; ipos++) cnt += t.h_m2l_tab[26 * (size_t)tt + ipos] >= 0;
         (cnt >= HAD_DENSE_MIN ? dense : sparse).push_back(tt);
+      }
+      // a group with few dense targets would leave most rows of the dense form's tiles (HADT_TT targets,
+      // one tile per frequency) empty; the round form packs its pairs into full rounds instead
+      if ((int)dense.size() < HAD_DENSE_GROUP_MIN) {
+        sparse.insert(sparse.end(), dense.begin(), dense.end());
+        std::sort(sparse.begin(), sparse.end());
+        dense.clear();
       }
       // dense targets level by level (node order within a level is Morton order): the targets of one
       // tile are then spatially compact and share most of their sources in L2
