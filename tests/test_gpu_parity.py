@@ -180,11 +180,12 @@ def test_hadamard_tcgen05_form(monkeypatch):
     assert pe < 5e-7 and ge < 5e-7, (pe, ge)
 
 
-# Orders beyond the fixtures: the slabbed real transforms at p = 9 (odd order: a partial last slab) and
-# p = 10 (the other occupancy setting), and the complex transforms at p = 9 and p = 12, against FP64
-# direct sums; the mixed path also against the FP64 path on the same tree.
-@pytest.mark.parametrize("kernel,p,wk", [("laplace", 9, 0.0), ("laplace", 10, 0.0),
-                                         ("helmholtz", 9, 20.0), ("helmholtz", 12, 20.0)])
+# Orders beyond the fixtures: the slabbed real transforms at p = 3 (one partial slab), p = 9 (odd order:
+# a partial last slab) and p = 10 (the other occupancy setting), and the complex transforms at p = 3, 9
+# and 12, against FP64 direct sums (bounded by the FMM's truncation error at that order); the mixed path
+# also against the FP64 path on the same tree.
+@pytest.mark.parametrize("kernel,p,wk", [("laplace", 3, 0.0), ("laplace", 9, 0.0), ("laplace", 10, 0.0),
+                                         ("helmholtz", 3, 5.0), ("helmholtz", 9, 20.0), ("helmholtz", 12, 20.0)])
 def test_high_orders_against_direct_sums(kernel, p, wk):
     rng = np.random.default_rng(11)
     n = 20000
@@ -202,7 +203,8 @@ def test_high_orders_against_direct_sums(kernel, p, wk):
     s = rng.choice(n, 300, replace=False)
     ex = orc.direct(kernel, x, q, x[s], wk)
     pe, ge = orc.rel_l2(outs["fp64"][s], ex)
-    assert pe < 1e-4 and ge < 1e-3, (pe, ge)        # bounded by the FMM's own truncation error
+    bound = 5e-2 if p == 3 else 1e-4                 # the FMM's own truncation error at this order
+    assert pe < bound and ge < 10 * bound, (pe, ge)
     pm, gm = orc.rel_l2(outs["mixed"], outs["fp64"])
     assert pm < 5e-6 and gm < 5e-6, (pm, gm)        # mixed precision against FP64 on the same tree
 
