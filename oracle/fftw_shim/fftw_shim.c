@@ -16,6 +16,7 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 typedef struct {
   double re, im;
@@ -259,10 +260,25 @@ static void exec_c2r(const struct xfmm_fft_plan_s* p, const double* in, double* 
   free(a);
 }
 
+/* Thread-seconds spent inside the transforms, summed over every calling thread, so that a caller can
+ * state how much of the reference's M2L stage this stand-in for FFTW accounts for. */
+static unsigned long long g_exec_ns = 0;
+
+static unsigned long long now_ns(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (unsigned long long)t.tv_sec * 1000000000ull + (unsigned long long)t.tv_nsec;
+}
+
+double xfmm_shim_exec_seconds(void) { return 1e-9 * (double)__atomic_load_n(&g_exec_ns, __ATOMIC_RELAXED); }
+void xfmm_shim_reset(void) { __atomic_store_n(&g_exec_ns, 0ull, __ATOMIC_RELAXED); }
+
 static void dispatch(const struct xfmm_fft_plan_s* p, const double* in, double* out) {
+  const unsigned long long t0 = now_ns();
   if (p->kind == KIND_C2C) exec_c2c(p, in, out);
   else if (p->kind == KIND_R2C) exec_r2c(p, in, out);
   else exec_c2r(p, in, out);
+  __atomic_fetch_add(&g_exec_ns, now_ns() - t0, __ATOMIC_RELAXED);
 }
 
 /* float entry points run the double transform on converted copies */
