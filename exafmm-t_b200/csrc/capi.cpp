@@ -92,6 +92,14 @@ xfmm_status xfmm_fmm_create(int kernel, int p, int ncrit, double k_re, double k_
   });
 }
 
+xfmm_status xfmm_fmm_set_operator_file(xfmm_fmm* fmm, const char* filename) {
+  return guarded([&] {
+    XREQUIRE(fmm, XFMM_ERR_ARG, "null argument");
+    fmm->f.filename = filename ? filename : "";
+    fmm->f.precomputed = false;  // the next precompute reads (or writes) the file
+  });
+}
+
 xfmm_status xfmm_fmm_free(xfmm_fmm* fmm) {
   return guarded([&] { delete fmm; });
 }
@@ -206,6 +214,7 @@ xfmm_status xfmm_get_values(xfmm_fmm* fmm, xfmm_tree* tree, double* out, int on_
       xfmm::get_values(fmm->f, tree->t, tree->t.stage_out.p, S(stream));
       XCUDA(cudaMemcpyAsync(out, tree->t.stage_out.p, n * sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
       XCUDA(cudaStreamSynchronize(S(stream)));
+      xfmm::check_device_status(fmm->f, tree->t);
     }
   });
 }
@@ -224,6 +233,7 @@ xfmm_status xfmm_evaluate(xfmm_fmm* fmm, xfmm_tree* tree, double* out, int on_de
       xfmm::get_values(fmm->f, tree->t, tree->t.stage_out.p, S(stream));
       XCUDA(cudaMemcpyAsync(out, tree->t.stage_out.p, n * sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
       XCUDA(cudaStreamSynchronize(S(stream)));
+      xfmm::check_device_status(fmm->f, tree->t);
     }
   });
 }

@@ -19,7 +19,6 @@
 //   M2P   fmm_base.h:97-124                              far part: k_eval (Laplace mixed: k_far_lap)
 //   P2P   fmm_base.h:82-94                               near part: k_near (Laplace mixed: k_near_lap_f2)
 // Results stay in tree order until get_values scatters them (python/exafmm.cpp:194-207).
-#include <cublas_v2.h>
 #include <cufft.h>
 
 #include <algorithm>
@@ -395,10 +394,6 @@ struct NearArgs {
   const double* src_qim;
   double* out;
   double k_re, k_im;
-  // Laplace paired-FP32 form: sources split once per evaluate into FP32 hi/lo parts relative to
-  // (ox, oy, oz), two float4 per source: {hx, hy, hz, q}, {lx, ly, lz, 0}
-  const float4* srcf;
-  double ox, oy, oz;
 };
 
 template <class R> struct Stage4;
@@ -559,19 +554,27 @@ __device__ __forceinline__ void near_leaf(const NearArgs& a, int node, int lane,
 // sm_100 paired FP32 operations (__ffma2_rn / __fadd2_rn / __fmul2_rn): the staged sources are laid
 // out structure-of-arrays so that sources (j, j+1) load as one float2, and the target's coordinates
 // are duplicated into both halves once per chunk.
-// Coordinates are split into FP32 hi + lo parts relative to one origin (the root centre) for the
-// whole evaluate: the separation (th - sh) + (tl - sl) is then accurate to a few FP32 ulps of itself
-// however close the pair is (the hi difference is rounded once, relative to its own size, and the lo
-// parts carry the residuals of both coordinates), so the sources are split once per evaluate
-// (k_src_split) instead of once per target leaf that stages them.
+// Coordinates are taken relative to the centre of the target leaf: each staged source is moved there in
+// FP64 and rounded to FP32 once per chunk (shared by every target of the warp), each target once, so a
+// pair's separation is a single FP32 subtraction of two values no larger than the 3 x 3 x 3 leaf
+// neighbourhood (a few leaf radii).  Its error is a few FP32 ulps of that neighbourhood's size, not of
+// the root's.  That is not enough for the closest pairs (the few pairs a few 1e-5 apart dominate the
+// gradient's norm over all targets), so every pair closer than NEAR_CLOSE x the leaf radius is left out
+// of the FP32 sums and computed again in FP64 from the bodies' FP64 coordinates, by the lanes that met
+// one, after the chunk.  Such pairs are rare (about 2% of the chunks at 4M bodies, p = 8, ncrit = 128),
+// and the error left in the FP32 pairs, ~2^-24 x (neighbourhood radius / separation), is then bounded
+// by separations above NEAR_CLOSE x the leaf radius.  Pairs at r == 0 in FP64 are skipped
+// (laplace.h:57).
+constexpr float NEAR_CLOSE = 0.125f;
 #ifndef XFMM_NEAR_CH
 #define XFMM_NEAR_CH 64
 #endif
 constexpr int NEAR_CH = XFMM_NEAR_CH;  // sources staged per chunk (32 or 64)
 static_assert(NEAR_CH == 32 || NEAR_CH == 64, "NEAR_CH");
 struct NearSmemF2 {
-  // source pair k = sources 2k, 2k+1: {hx, hy}, {hz, q}, {lx, ly}, {lz, -} as float2 pairs
-  float4 pr[NEAR_CH / 2][4];
+  // source pair k = sources 2k, 2k+1 relative to the leaf centre: {x, x'}, {y, y'} and {z, z'}, {q, q'}
+  float4 pr[NEAR_CH / 2][2];
+  int64_t sidx[NEAR_CH];  // the chunk's sources in src4 (-1: padding)
   int64_t seg_beg[NEAR_SEG];
   int seg_pre[NEAR_SEG + 1];
 };
@@ -583,39 +586,36 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
   const int T = a.ntrgs[node];
   const int64_t tb = a.tbeg[node];
   const int64_t e0 = a.p2p_off[node], e1 = a.p2p_off[node + 1];
+  const double4 cn = a.center[node];
   int G2 = 1;  // at most 16 lanes per target
   if (TPL == 1)
     while (G2 * 2 * T <= 32 && G2 < 16) G2 *= 2;
   const int tl = lane / G2, sub = lane % G2;
   const int npl = NEAR_CH / 2 / G2;  // source pairs per lane per chunk
   const float2 M1 = make_float2(-1.f, -1.f);
+  const float dc2 = (float)(NEAR_CLOSE * cn.w) * (float)(NEAR_CLOSE * cn.w);  // close-pair threshold, squared
   for (int t0 = 0; t0 < T; t0 += 32 * TPL) {
-    float2 TX[TPL], TY[TPL], TZ[TPL], LX[TPL], LY[TPL], LZ[TPL];
+    float2 TX[TPL], TY[TPL], TZ[TPL];
     double P[TPL], GX[TPL], GY[TPL], GZ[TPL];
 #pragma unroll
     for (int u = 0; u < TPL; u++) {
       const int t = t0 + tl + 32 * u;
-      double dx = 0, dy = 0, dz = 0;
+      float x = 0.f, y = 0.f, z = 0.f;
       if (t < T) {
         const double4 v = a.trg4[tb + t];
-        dx = v.x - a.ox;
-        dy = v.y - a.oy;
-        dz = v.z - a.oz;
+        x = (float)(v.x - cn.x);
+        y = (float)(v.y - cn.y);
+        z = (float)(v.z - cn.z);
       }
-      const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
-      TX[u] = dup2(hx);
-      TY[u] = dup2(hy);
-      TZ[u] = dup2(hz);
-      LX[u] = dup2((float)(dx - (double)hx));
-      LY[u] = dup2((float)(dy - (double)hy));
-      LZ[u] = dup2((float)(dz - (double)hz));
+      TX[u] = dup2(x);
+      TY[u] = dup2(y);
+      TZ[u] = dup2(z);
       P[u] = GX[u] = GY[u] = GZ[u] = 0.0;
     }
     for (int64_t eb = e0; eb < e1; eb += NEAR_SEG) {
       const int nseg = (int)(e1 - eb < NEAR_SEG ? e1 - eb : NEAR_SEG);
       __syncwarp();
       int carry = 0;
-      int own_b = -1, own_e = -1;  // stream positions of the leaf's own sources in this batch
       for (int k0 = 0; k0 < nseg; k0 += 32) {
         const int k = k0 + lane;
         int cnt = 0, sn = -1;
@@ -631,12 +631,6 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
           if (lane >= o) incl += v;
         }
         if (k < nseg) sm.seg_pre[k + 1] = carry + incl;
-        const unsigned om = __ballot_sync(0xffffffffu, sn == node);
-        if (om) {
-          const int l = __ffs(om) - 1;
-          own_e = carry + __shfl_sync(0xffffffffu, incl, l);
-          own_b = own_e - __shfl_sync(0xffffffffu, cnt, l);
-        }
         carry += __shfl_sync(0xffffffffu, incl, 31);
       }
       if (lane == 0) sm.seg_pre[0] = 0;
@@ -648,53 +642,50 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
 #pragma unroll
         for (int h = 0; h < NEAR_CH / 32; h++) {
           const int pos = p0 + 32 * h + lane;
-          // zero-charge padding: contributes 0 wherever it lies (r == 0 is masked below)
-          float4 hi = make_float4(0.f, 0.f, 0.f, 0.f), lo = hi;
+          // zero-charge padding far away: contributes 0 and never counts as close
+          float x = 1e18f, y = 1e18f, z = 1e18f, q = 0.f;
+          int64_t si = -1;
           if (pos < total) {
             while (sm.seg_pre[seg + 1] <= pos) seg++;
-            const int64_t si = sm.seg_beg[seg] + (pos - sm.seg_pre[seg]);
-            hi = a.srcf[2 * si];
-            lo = a.srcf[2 * si + 1];
+            si = sm.seg_beg[seg] + (pos - sm.seg_pre[seg]);
+            const double4 v = a.src4[si];
+            x = (float)(v.x - cn.x);
+            y = (float)(v.y - cn.y);
+            z = (float)(v.z - cn.z);
+            q = (float)v.w;
           }
+          sm.sidx[32 * h + lane] = si;
           float* r = reinterpret_cast<float*>(sm.pr[16 * h + (lane >> 1)]) + (lane & 1);  // float2 slot
-          r[0] = hi.x;
-          r[2] = hi.y;
-          r[4] = hi.z;
-          r[6] = hi.w;
-          r[8] = lo.x;
-          r[10] = lo.y;
-          r[12] = lo.z;
+          r[0] = x;
+          r[2] = y;
+          r[4] = z;
+          r[6] = q;
         }
         __syncwarp();
         float2 p2[TPL], gx2[TPL], gy2[TPL], gz2[TPL];
 #pragma unroll
         for (int u = 0; u < TPL; u++) p2[u] = gx2[u] = gy2[u] = gz2[u] = make_float2(0.f, 0.f);
-        // r == 0 (a target meeting itself or a duplicate point; both lie in the leaf's own sources) and
-        // the zero-charge padding (the stream's last chunk) need the mask; the other chunks skip it
-        auto pairs = [&](auto masked) {
+        // pairs closer than the threshold (r == 0 among them) are left out here and redone below; bit jj
+        // of `cm` marks the lane's source pair jj as holding one
+        uint32_t cm = 0;
 #pragma unroll 4
         for (int jj = 0; jj < npl; jj++) {
+          bool cl = false;
           const int jp = jj * G2 + sub;  // source pair
-          const float4 A0 = sm.pr[jp][0], A1 = sm.pr[jp][1], A2 = sm.pr[jp][2], A3 = sm.pr[jp][3];
-          const float2 HX = make_float2(A0.x, A0.y), HY = make_float2(A0.z, A0.w);
-          const float2 HZ = make_float2(A1.x, A1.y), Q = make_float2(A1.z, A1.w);
-          const float2 SX = make_float2(A2.x, A2.y), SY = make_float2(A2.z, A2.w);
-          const float2 SZ = make_float2(A3.x, A3.y);
+          const float4 A0 = sm.pr[jp][0], A1 = sm.pr[jp][1];
+          const float2 SX = make_float2(A0.x, A0.y), SY = make_float2(A0.z, A0.w);
+          const float2 SZ = make_float2(A1.x, A1.y), Q = make_float2(A1.z, A1.w);
 #pragma unroll
           for (int u = 0; u < TPL; u++) {
-            // separation (t - s) from hi and lo parts
-            const float2 dx = __fadd2_rn(__ffma2_rn(HX, M1, TX[u]), __ffma2_rn(SX, M1, LX[u]));
-            const float2 dy = __fadd2_rn(__ffma2_rn(HY, M1, TY[u]), __ffma2_rn(SY, M1, LY[u]));
-            const float2 dz = __fadd2_rn(__ffma2_rn(HZ, M1, TZ[u]), __ffma2_rn(SZ, M1, LZ[u]));
+            const float2 dx = __ffma2_rn(SX, M1, TX[u]);  // t - s
+            const float2 dy = __ffma2_rn(SY, M1, TY[u]);
+            const float2 dz = __ffma2_rn(SZ, M1, TZ[u]);
             float2 r2 = __fmul2_rn(dx, dx);
             r2 = __ffma2_rn(dy, dy, r2);
             r2 = __ffma2_rn(dz, dz, r2);
-            float ia = rsqrtf(r2.x), ib = rsqrtf(r2.y);
-            if constexpr (decltype(masked)::value) {
-              ia = r2.x > 0.f ? ia : 0.f;  // r == 0 contributes nothing (laplace.h:57)
-              ib = r2.y > 0.f ? ib : 0.f;
-            }
-            const float2 inv = make_float2(ia, ib);
+            const bool fa = r2.x > dc2, fb = r2.y > dc2;
+            cl |= !(fa && fb);
+            const float2 inv = make_float2(fa ? rsqrtf(r2.x) : 0.f, fb ? rsqrtf(r2.y) : 0.f);
             const float2 qi = __fmul2_rn(Q, inv);
             const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
             p2[u] = __fadd2_rn(p2[u], qi);
@@ -702,16 +693,49 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
             gy2[u] = __ffma2_rn(qi3, dy, gy2[u]);
             gz2[u] = __ffma2_rn(qi3, dz, gz2[u]);
           }
+          if (cl) cm |= 1u << jj;
         }
-        };
-        if (p0 + NEAR_CH > total || (own_b < p0 + NEAR_CH && own_e > p0)) pairs(std::true_type());
-        else pairs(std::false_type());
 #pragma unroll
         for (int u = 0; u < TPL; u++) {
           P[u] += (double)(p2[u].x + p2[u].y);
           GX[u] -= (double)(gx2[u].x + gx2[u].y);
           GY[u] -= (double)(gy2[u].x + gy2[u].y);
           GZ[u] -= (double)(gz2[u].x + gz2[u].y);
+        }
+        while (cm) {  // the lane's close pairs, in FP64 (the same FP32 test picks them out)
+          {
+            const int jj = __ffs(cm) - 1;
+            cm &= cm - 1;
+            const int jp = jj * G2 + sub;
+            const float4 A0 = sm.pr[jp][0], A1 = sm.pr[jp][1];
+            const float2 SX = make_float2(A0.x, A0.y), SY = make_float2(A0.z, A0.w);
+            const float2 SZ = make_float2(A1.x, A1.y);
+#pragma unroll
+            for (int u = 0; u < TPL; u++) {
+              const int t = t0 + tl + 32 * u;
+              if (t >= T) continue;
+              const float2 dx = __ffma2_rn(SX, M1, TX[u]);
+              const float2 dy = __ffma2_rn(SY, M1, TY[u]);
+              const float2 dz = __ffma2_rn(SZ, M1, TZ[u]);
+              float2 r2 = __fmul2_rn(dx, dx);
+              r2 = __ffma2_rn(dy, dy, r2);
+              r2 = __ffma2_rn(dz, dz, r2);
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                const int64_t si = sm.sidx[2 * jp + h];
+                if ((h == 0 ? r2.x : r2.y) > dc2 || si < 0) continue;
+                const double4 tv = a.trg4[tb + t], sv = a.src4[si];
+                const double ex = tv.x - sv.x, ey = tv.y - sv.y, ez = tv.z - sv.z;
+                const double e2 = ex * ex + ey * ey + ez * ez;
+                if (e2 == 0.0) continue;  // r == 0 contributes nothing (laplace.h:57)
+                const double ir = rsqrt(e2), qi = sv.w * ir, qi3 = qi * ir * ir;
+                P[u] += qi;
+                GX[u] -= qi3 * ex;
+                GY[u] -= qi3 * ey;
+                GZ[u] -= qi3 * ez;
+              }
+            }
+          }
         }
       }
     }
@@ -925,92 +949,7 @@ __global__ void __launch_bounds__(128) k_surf_pot_lap_f2(SurfPotArgs a) {
   }
 }
 
-// ================================================================ translation GEMMs
-// Row gather / scatter around the library GEMMs: the rows of an operator application live at scattered
-// offsets (leaf and node rows of up/dn/chk/eq), the GEMMs want them contiguous.
-//   gather:  dst[r][j]           = alpha_r * src[aoff[r] + j]   (scaled in the destination type)
-//   scatter: dst[coff[r] + j] (+)= alpha_r * src[r][j]          (scaled in the source type)
-template <class TS, class TD>
-__global__ void k_rows_gather(int m, int n, const TS* __restrict__ src, const int64_t* __restrict__ aoff,
-                              const double* __restrict__ alpha, TD* __restrict__ dst) {
-  const int64_t total = (int64_t)m * n;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int r = (int)(e / n), j = (int)(e - (int64_t)r * n);
-    TD v = cvt<TD>(src[aoff[r] + j]);
-    if (alpha) v = vscale(v, (typename Base<TD>::type)alpha[r]);
-    dst[e] = v;
-  }
-}
-template <class TS, class TD>
-__global__ void k_rows_scatter(int m, int n, const TS* __restrict__ src, const int64_t* __restrict__ coff,
-                               const double* __restrict__ alpha, TD* __restrict__ dst, int accumulate) {
-  const int64_t total = (int64_t)m * n;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int r = (int)(e / n), j = (int)(e - (int64_t)r * n);
-    TS v = src[e];
-    if (alpha) v = vscale(v, (typename Base<TS>::type)alpha[r]);
-    TD* d = dst + coff[r] + j;
-    *d = accumulate ? vadd(*d, cvt<TD>(v)) : cvt<TD>(v);
-  }
-}
-inline int rows_grid(int64_t total) { return (int)std::min<int64_t>(nblk(total), 148 * 16); }
-// Columns of y = B1^T c kept for e = B2 y: the pinv rank rounded up to a multiple of 8 (at most n), so
-// that rows of y start 64-byte aligned and the library picks its aligned (tensor-core) GEMM kernels.
-// Exact: the B2 rows past the rank are zero.
-inline int pinv_cols(int rank, int n) { return std::min(n, (rank + 7) & ~7); }
-__global__ void k_to_double(const float* __restrict__ in, int64_t n, double* __restrict__ out) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
-    out[e] = (double)in[e];
-}
-
-
-#define XCUBLAS2(call)                                                                               \
-  do {                                                                                               \
-    cublasStatus_t st_ = (call);                                                                     \
-    if (st_ != CUBLAS_STATUS_SUCCESS)                                                                \
-      throw Error(XFMM_ERR_CUDA, std::string("cuBLAS ") + #call + " failed: " + std::to_string((int)st_)); \
-  } while (0)
-
-// Row-major C[m][n] = A[m][k] B[k][n] with the library GEMM (column-major: C^T = B^T A^T).
-inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const float* A, const float* B, float* C) {
-  const float one = 1.f, zero = 0.f;
-  XCUBLAS2(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, B, n, A, k, &zero, C, n));
-}
-inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const double* A, const double* B, double* C) {
-  const double one = 1.0, zero = 0.0;
-  XCUBLAS2(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, B, n, A, k, &zero, C, n));
-}
-inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const float2* A, const float2* B, float2* C) {
-  const cuComplex one = make_cuComplex(1.f, 0.f), zero = make_cuComplex(0.f, 0.f);
-  XCUBLAS2(cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, (const cuComplex*)B, n, (const cuComplex*)A, k,
-                       &zero, (cuComplex*)C, n));
-}
-inline void gemm_rm(cublasHandle_t h, int m, int n, int k, const double2* A, const double2* B, double2* C) {
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
-  XCUBLAS2(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, (const cuDoubleComplex*)B, n,
-                       (const cuDoubleComplex*)A, k, &zero, (cuDoubleComplex*)C, n));
-}
-
-// Row-major C[m][n] = A[m][k] B[k][n] with leading dimensions (rows of A, B, C lda, ldb, ldc apart).
-inline void gemm_rm_ld(cublasHandle_t h, int m, int n, int k, const float* A, int lda, const float* B, int ldb,
-                       float* C, int ldc) {
-  const float one = 1.f, zero = 0.f;
-  XCUBLAS2(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, B, ldb, A, lda, &zero, C, ldc));
-}
-inline void gemm_rm_ld(cublasHandle_t h, int m, int n, int k, const double* A, int lda, const double* B, int ldb,
-                       double* C, int ldc) {
-  const double one = 1.0, zero = 0.0;
-  XCUBLAS2(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, B, ldb, A, lda, &zero, C, ldc));
-}
-inline void gemm_rm_ld(cublasHandle_t h, int m, int n, int k, const double2* A, int lda, const double2* B, int ldb,
-                       double2* C, int ldc) {
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
-  XCUBLAS2(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &one, (const cuDoubleComplex*)B, ldb,
-                       (const cuDoubleComplex*)A, lda, &zero, (cuDoubleComplex*)C, ldc));
-}
-
-// ================================================================ M2L
-// grid[(s*8 + c)*nconv + g] = up[child c of source s][surface point mapped to g] (0 elsewhere)
+// ================================================================ M2L grid fallback (cuFFT, p beyond the DFT kernels)
 template <class W>
 __global__ void k_m2l_grid_up(const int* __restrict__ src, int nsrc, const int* __restrict__ child0,
                               const W* __restrict__ up, int nsurf, const int* __restrict__ conv2surf, int nconv,
@@ -2224,16 +2163,6 @@ __global__ void k_m2l_gather_dn(const int* __restrict__ trg, int ntrg, const int
 
 // ================================================================ misc
 // Sources of the Laplace paired-FP32 near field: hi/lo FP32 parts of (x - o), FP32 charge.
-__global__ void k_src_split(const double4* __restrict__ src4, int64_t n, double ox, double oy, double oz,
-                            float4* __restrict__ srcf) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double4 v = src4[i];
-  const double dx = v.x - ox, dy = v.y - oy, dz = v.z - oz;
-  const float hx = (float)dx, hy = (float)dy, hz = (float)dz;
-  srcf[2 * i] = make_float4(hx, hy, hz, (float)v.w);
-  srcf[2 * i + 1] = make_float4((float)(dx - (double)hx), (float)(dy - (double)hy), (float)(dz - (double)hz), 0.f);
-}
 // *bad becomes nonzero if any of v[0, n) is NaN or infinite
 __global__ void k_count_nonfinite(const double* __restrict__ v, int64_t n, int* __restrict__ bad) {
   int found = 0;
@@ -2264,6 +2193,8 @@ __global__ void k_scatter_out(const double* __restrict__ in, const int* __restri
 }  // namespace
 
 // ================================================================ workspace
+// Rows of one batch of translation GEMMs (translate.cu): per row its A and C offsets in real elements of
+// the buffers (complex values count twice) and its scale.
 struct GemmRows {
   int M = 0;
   DBuf<int64_t> a, c;
@@ -2274,14 +2205,9 @@ struct Workspace {
   int precision = -1, kernel = -1, p = 0;
   size_t vsz = 0;
   DBuf<char> up, dn, chk;  // working precision
-  DBuf<char> ybuf, eq;     // FP64: pinv intermediate, downward equivalent densities of the leaves
-  DBuf<char> xbuf;         // FP64: pinv input rows / output rows (contiguous, in leaf-level order)
-  DBuf<char> wA, wC;       // working precision: M2M/L2L input and output rows (contiguous)
-  cublasHandle_t blas = nullptr;
-  DBuf<char> blas_ws;      // the library GEMMs' workspace, fixed at creation (no allocation while capturing)
-  bool sgemm_emulated = false;  // FP32 GEMMs on the tensor cores (BF16x9 emulation)
+  DBuf<char> ybuf, eq;     // FP64: pinv intermediate (rows of the kept singular directions), downward
+                           // equivalent densities of the leaves
   DBuf<double> out;
-  DBuf<float4> srcf;  // Laplace mixed near field: per source {hx, hy, hz, q}, {lx, ly, lz, 0}
   DBuf<int> status;   // set by a kernel whose bounded wait ran out (0: none)
   // leaves grouped by level (P2M / L2P operators are per level except for Laplace)
   std::vector<int> leaf_level_off;
@@ -2319,7 +2245,6 @@ struct Workspace {
   std::vector<cudaEvent_t> m2l_ev;  // 4 per M2L group
   bool ev_ok = false;
   ~Workspace() {
-    if (blas) cublasDestroy(blas);
     for (auto h : fwd) cufftDestroy(h);
     for (auto h : bwd) cufftDestroy(h);
     if (ev_ok) {
@@ -2364,18 +2289,6 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   W.chk.alloc((size_t)std::max(t.nleafs, 1) * n * W.vsz);
   W.ybuf.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
   W.eq.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
-  W.xbuf.alloc((size_t)std::max(t.nleafs, 1) * n * 8 * (cplx ? 2 : 1));
-  XCUBLAS2(cublasCreate(&W.blas));
-  W.blas_ws.alloc((size_t)32 << 20);
-  XCUBLAS2(cublasSetWorkspace(W.blas, W.blas_ws.p, W.blas_ws.bytes()));
-#ifndef XFMM_SGEMM_BF16X9
-#define XFMM_SGEMM_BF16X9 1
-#endif
-  // FP32 translation GEMMs (M2M, L2L of the mixed path) run as the library's FP32 emulation on the
-  // tensor cores (three BF16 terms per operand, FP32 accuracy) where the loaded cuBLAS has it (12.9 and
-  // later); an older cuBLAS already loaded into the process keeps its default FP32 GEMMs
-  if (XFMM_SGEMM_BF16X9 && f.mixed())
-    W.sgemm_emulated = cublasSetMathMode(W.blas, CUBLAS_FP32_EMULATED_BF16X9_MATH) == CUBLAS_STATUS_SUCCESS;
   W.out.alloc((size_t)t.ntrg * 4 * (cplx ? 2 : 1));
   W.status.alloc(1);
   {
@@ -2383,7 +2296,6 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
     W.had_tc5 = e && e[0] == '1';
   }
   XCUDA(cudaMemsetAsync(W.status.p, 0, sizeof(int), s));
-  if (f.kernel == XFMM_LAPLACE && f.mixed()) W.srcf.alloc(2 * (size_t)std::max<int64_t>(t.nsrc, 1));
   // leaf rows grouped by level: P2M (chk[pos] -> up[node]) and L2P (dn[node] -> eq[pos])
   const bool lap = f.kernel == XFMM_LAPLACE;
   std::vector<int> order(t.nleafs);
@@ -2400,10 +2312,11 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
       while (cur < t.nleafs && t.h_level[t.h_leafs[order[cur]]] == l) cur++;
     }
     W.leaf_level_off[t.depth + 1] = cur;
+    const int64_t rn = (int64_t)n * (cplx ? 2 : 1);  // row length in real elements
     for (int i : order) {
       const int node = t.h_leafs[i];
-      idn.push_back((int64_t)i * n);
-      nodes.push_back((int64_t)node * n);
+      idn.push_back((int64_t)i * rn);
+      nodes.push_back((int64_t)node * rn);
       al.push_back(lap ? std::pow(0.5, t.h_level[node]) : 1.0);
       one.push_back(1.0);
     }
@@ -2422,20 +2335,15 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
     std::vector<double> one;
     for (int k : t.h_nonleafs)
       if (t.h_level[k] == l) {
-        ma.push_back((int64_t)t.h_child0[k] * n);
-        mc.push_back((int64_t)k * n);
-        la.push_back((int64_t)k * n);
-        lc.push_back((int64_t)t.h_child0[k] * n);
+        const int64_t rn = (int64_t)n * (cplx ? 2 : 1);
+        ma.push_back((int64_t)t.h_child0[k] * rn);
+        mc.push_back((int64_t)k * rn);
+        la.push_back((int64_t)k * rn);
+        lc.push_back((int64_t)t.h_child0[k] * rn);
         one.push_back(1.0);
       }
     upload_rows<double>(W.m2m[l], ma, mc, one, s);
     upload_rows<double>(W.l2l[l], la, lc, one, s);
-  }
-  {
-    int maxp = 1;
-    for (int l = 0; l <= t.depth; l++) maxp = std::max(maxp, W.m2m[l].M);
-    W.wA.alloc((size_t)maxp * 8 * n * W.vsz);
-    W.wC.alloc((size_t)maxp * 8 * n * W.vsz);
   }
   // M2L buffers and FFT plans
   const int ng = (int)t.m2l_src_off.size() - 1;
@@ -2602,20 +2510,7 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
   return W;
 }
 
-template <class W, class V64>
-struct Ops {
-  const V64 *p2m1, *p2m2, *l2p1, *l2p2;  // FP64 check-to-equivalent factors
-  const W *m2m, *l2l;                   // working precision
-};
-template <class W, class V64>
-Ops<W, V64> ops_of(const Fmm& f, int level) {
-  const LevelOps& o = f.ops[f.kernel == XFMM_LAPLACE ? 0 : level];
-  return Ops<W, V64>{(const V64*)o.p2m_B1.p, (const V64*)o.p2m_B2.p, (const V64*)o.l2p_B1.p,
-                     (const V64*)o.l2p_B2.p, (const W*)o.m2m_B.p,     (const W*)o.l2l_B.p};
-}
-
-template <class RB> const RB* alpha_of(const GemmRows& g);
-template <> const double* alpha_of<double>(const GemmRows& g) { return g.al64.p; }
+inline const LevelOps& level_ops(const Fmm& f, int level) { return f.ops[f.kernel == XFMM_LAPLACE ? 0 : level]; }
 
 template <class RB> const RB* m2l_scale_of(const Tree& t);
 template <> const float* m2l_scale_of<float>(const Tree& t) { return t.m2l_scale.p; }
@@ -2627,6 +2522,7 @@ struct Engine {
   using W = typename Green<KER, R>::Q;          // working value: R or complex
   using V64 = typename Green<KER, double>::Q;   // FP64 value (pinv GEMMs, downward equivalent densities)
   using CT = typename C2<R>::type;              // spectrum value
+  static constexpr int CW = KER == K_HELMHOLTZ ? 2 : 1;  // reals per value
 
   static void upward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s) {
     const int n = f.nsurf;
@@ -2642,50 +2538,40 @@ struct Engine {
         k_surf_pot<KER, R><<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
       XLAUNCH();
       ws.launches++;
-      W* up = (W*)ws.up.p;
-      V64* X = (V64*)ws.xbuf.p;
-      V64* Y = (V64*)ws.ybuf.p;
-      XCUBLAS2(cublasSetStream(ws.blas, s));
+      // e = 0.5^l (V S+) (U^H c) per leaf level, two FP64 GEMMs on the tensor cores: y over the kept
+      // singular directions only, then e scattered to the leaves' up rows with the level's scale.
+      // (An FP32 first factor, as in L2P below, measured 1.4e-7 more potential error at p = 8 and 3e-7
+      // at p = 10: the upward densities feed every later translation.)
       for (int l = 0; l <= t.depth; l++) {
         if (KER == K_LAPLACE && l > 0) break;
         const int r0 = ws.leaf_level_off[l], r1 = ws.leaf_level_off[l + 1];
         const int m = KER == K_LAPLACE ? ws.p2m1.M : r1 - r0;
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
-        const Ops<W, V64> o = ops_of<W, V64>(f, l);
-        // rows of this leaf level, contiguous in FP64; e = (V S+) (U^H c) in two FP64 GEMMs; scaled scatter.
-        // (An FP32 first factor, as in L2P below, measured 1.4e-7 more potential error at p = 8 and 3e-7
-        // at p = 10: the upward densities feed every later translation.)
-        const int64_t tot = (int64_t)m * n;
-        k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.chk.p, ws.p2m1.a.p + off, nullptr,
-                                                            X + (int64_t)off * n);
-        XLAUNCH();
-        // y = U^H c over the kept singular directions only (rank r <= n), then e = V S+ y
-        const int r = pinv_cols(f.ops[KER == K_LAPLACE ? 0 : l].rank, n);
-        gemm_rm_ld(ws.blas, m, r, n, X + (int64_t)off * n, n, o.p2m1, n, Y + (int64_t)off * n, r);
-        gemm_rm_ld(ws.blas, m, n, r, Y + (int64_t)off * n, r, o.p2m2, n, X + (int64_t)off * n, n);
-        k_rows_scatter<V64, W><<<rows_grid(tot), 256, 0, s>>>(m, n, X + (int64_t)off * n, ws.p2m2.c.p + off,
-                                                             alpha_of<double>(ws.p2m2) + off, up, 0);
-        XLAUNCH();
+        const LevelOps& op = level_ops(f, l);
+        const int rk = op.rank;
+        TGemm g1{m, CW * rk, CW * n, ws.p2m1.a.p + off, ws.p2m1.c.p + off, nullptr, (int64_t)CW * n, 0, (int64_t)CW * n};
+        tgemm_f64<R, double>(g1, (const R*)ws.chk.p, op.tg_p2m1.p, (double*)ws.ybuf.p, s);
+        TGemm g2{m, CW * n, CW * rk, ws.p2m2.a.p + off, ws.p2m2.c.p + off, ws.p2m2.al64.p + off, (int64_t)CW * n, 0,
+                 (int64_t)CW * n};
+        tgemm_f64<double, R>(g2, (const double*)ws.ybuf.p, op.tg_p2m2.p, (R*)ws.up.p, s);
         ws.launches += 2;
       }
     }
     XCUDA(cudaEventRecord(ws.ev[1], s));
-    // M2M: deepest parents first (post-order); per level the parents' 8 children rows (contiguous per
-    // parent) gathered, one GEMM with the [8n][n] operator, the results scattered to the parents
-    XCUBLAS2(cublasSetStream(ws.blas, s));
+    // M2M: deepest parents first (post-order); per level one GEMM of the parents' 8 children rows
+    // (contiguous per parent) with the [8n][n] operator, written to the parents' rows
     for (int l = t.depth - 1; l >= 0; l--) {
       const GemmRows& g = ws.m2m[l];
       if (g.M <= 0) continue;
-      const int64_t tot = (int64_t)g.M * 8 * n;
-      k_rows_gather<W, W><<<rows_grid(tot), 256, 0, s>>>(g.M, 8 * n, (const W*)ws.up.p, g.a.p, nullptr,
-                                                        (W*)ws.wA.p);
-      XLAUNCH();
-      gemm_rm(ws.blas, g.M, n, 8 * n, (const W*)ws.wA.p, ops_of<W, V64>(f, l).m2m, (W*)ws.wC.p);
-      k_rows_scatter<W, W><<<rows_grid((int64_t)g.M * n), 256, 0, s>>>(g.M, n, (const W*)ws.wC.p, g.c.p, nullptr,
-                                                                      (W*)ws.up.p, 0);
-      XLAUNCH();
-      ws.launches += 2;
+      const LevelOps& op = level_ops(f, l);
+      TGemm gm{g.M, CW * n, CW * 8 * n, g.a.p, g.c.p, nullptr, (int64_t)CW * n, 0, (int64_t)CW * n};
+      gm.status = ws.status.p;
+      if constexpr (sizeof(R) == 4)
+        tgemm_tc<float>(gm, (const float*)ws.up.p, op.tg_m2m_h.p, op.tg_m2m_l.p, op.ld_m2m, (float*)ws.up.p, s);
+      else
+        tgemm_f64<double, double>(gm, (const double*)ws.up.p, op.tg_m2m.p, (double*)ws.up.p, s);
+      ws.launches++;
     }
     XCUDA(cudaEventRecord(ws.ev[2], s));
   }
@@ -2897,60 +2783,45 @@ struct Engine {
     // M2L
     if (t.n_m2l_trg) m2l(f, t, ws, s);
     XCUDA(cudaEventRecord(ws.ev[4], s));
-    // L2L: shallowest parents first (pre-order); per level the parents' rows gathered, one GEMM with the
-    // [n][8n] operator, the results added to the 8 children rows (contiguous per parent)
-    XCUBLAS2(cublasSetStream(ws.blas, s));
+    // L2L: shallowest parents first (pre-order); per level one GEMM of the parents' rows with the
+    // [n][8n] operator, added to the 8 children rows (contiguous per parent)
     for (int l = 0; l < t.depth; l++) {
       const GemmRows& g = ws.l2l[l];
       if (g.M <= 0) continue;
-      k_rows_gather<W, W><<<rows_grid((int64_t)g.M * n), 256, 0, s>>>(g.M, n, (const W*)ws.dn.p, g.a.p, nullptr,
-                                                                      (W*)ws.wA.p);
-      XLAUNCH();
-      gemm_rm(ws.blas, g.M, 8 * n, n, (const W*)ws.wA.p, ops_of<W, V64>(f, l).l2l, (W*)ws.wC.p);
-      k_rows_scatter<W, W><<<rows_grid((int64_t)g.M * 8 * n), 256, 0, s>>>(g.M, 8 * n, (const W*)ws.wC.p, g.c.p,
-                                                                          nullptr, (W*)ws.dn.p, 1);
-      XLAUNCH();
-      ws.launches += 2;
+      const LevelOps& op = level_ops(f, l);
+      TGemm gl{g.M, CW * 8 * n, CW * n, g.a.p, g.c.p, nullptr, (int64_t)CW * 8 * n, 1, (int64_t)CW * n};
+      gl.status = ws.status.p;
+      if constexpr (sizeof(R) == 4)
+        tgemm_tc<float>(gl, (const float*)ws.dn.p, op.tg_l2l_h.p, op.tg_l2l_l.p, op.ld_l2l, (float*)ws.dn.p, s);
+      else
+        tgemm_f64<double, double>(gl, (const double*)ws.dn.p, op.tg_l2l.p, (double*)ws.dn.p, s);
+      ws.launches++;
     }
     XCUDA(cudaEventRecord(ws.ev[5], s));
-    // L2P part 1: downward check -> equivalent (DC2E) per leaf level: leaf rows gathered in FP64 with
-    // their scale, e = conj(U) S+ (conj(VH) c) in two FP64 GEMMs, scattered to the leaf positions
+    // L2P part 1: downward check -> equivalent (DC2E) per leaf level, e = conj(U) S+ (conj(VH) 0.5^l c):
+    // y over the kept singular directions, then e to the leaf positions (FP64).
     if (t.nleafs) {
-      V64* X = (V64*)ws.xbuf.p;
-      V64* Y = (V64*)ws.ybuf.p;
       for (int l = 0; l <= t.depth; l++) {
         if (KER == K_LAPLACE && l > 0) break;
         const int r0 = ws.leaf_level_off[l], r1 = ws.leaf_level_off[l + 1];
         const int m = KER == K_LAPLACE ? ws.l2p1.M : r1 - r0;
         const int off = KER == K_LAPLACE ? 0 : r0;
         if (m <= 0) continue;
-        const Ops<W, V64> o = ops_of<W, V64>(f, l);
-        const int64_t tot = (int64_t)m * n;
-        const int r = pinv_cols(f.ops[KER == K_LAPLACE ? 0 : l].rank, n);
+        const LevelOps& op = level_ops(f, l);
+        const int rk = op.rank;
+        TGemm g1{m, CW * rk, CW * n, ws.l2p1.a.p + off, ws.l2p1.c.p + off, ws.l2p2.al64.p + off, (int64_t)CW * n, 0,
+                 (int64_t)CW * n};
         // The mixed path's downward check values are FP32 and conj(VH) is orthogonal: y = conj(VH) c runs
-        // in FP32 (the library's tensor-core emulation where it has it) inside this level's FP64 row block,
-        // then y moves to FP64 for e = conj(U) S+ y, whose 1/s amplification needs FP64.  These densities
-        // feed only the leaf's own targets (measured: +0.5e-7 potential error at p = 8, +1e-7 at p = 10).
-        if constexpr (sizeof(W) == 4) {
-          float* Xf = reinterpret_cast<float*>(X + (int64_t)off * n);
-          float* Yf = Xf + tot;
-          k_rows_gather<W, float><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.dn.p, ws.l2p1.a.p + off,
-                                                                alpha_of<double>(ws.l2p2) + off, Xf);
-          XLAUNCH();
-          gemm_rm_ld(ws.blas, m, r, n, Xf, n, (const float*)f.ops[KER == K_LAPLACE ? 0 : l].l2p_B1f.p, n, Yf, r);
-          k_to_double<<<rows_grid((int64_t)m * r), 256, 0, s>>>(Yf, (int64_t)m * r, Y + (int64_t)off * n);
-          XLAUNCH();
-          ws.launches++;
-        } else {
-          k_rows_gather<W, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, (const W*)ws.dn.p, ws.l2p1.a.p + off,
-                                                              alpha_of<double>(ws.l2p2) + off, X + (int64_t)off * n);
-          XLAUNCH();
-          gemm_rm_ld(ws.blas, m, r, n, X + (int64_t)off * n, n, o.l2p1, n, Y + (int64_t)off * n, r);
-        }
-        gemm_rm_ld(ws.blas, m, n, r, Y + (int64_t)off * n, r, o.l2p2, n, X + (int64_t)off * n, n);
-        k_rows_scatter<V64, V64><<<rows_grid(tot), 256, 0, s>>>(m, n, X + (int64_t)off * n, ws.l2p2.c.p + off,
-                                                               nullptr, (V64*)ws.eq.p, 0);
-        XLAUNCH();
+        // at FP32 accuracy (TF32 x 3), then e = conj(U) S+ y, whose 1/s amplification needs FP64.  These
+        // densities feed only the leaf's own targets (measured: +0.5e-7 potential error at p = 8, +1e-7
+        // at p = 10).
+        g1.status = ws.status.p;
+        if constexpr (sizeof(R) == 4 && KER != K_HELMHOLTZ)
+          tgemm_tc<double>(g1, (const float*)ws.dn.p, op.tg_l2p1_h.p, op.tg_l2p1_l.p, op.ld_l2p1, (double*)ws.ybuf.p, s);
+        else
+          tgemm_f64<R, double>(g1, (const R*)ws.dn.p, op.tg_l2p1.p, (double*)ws.ybuf.p, s);
+        TGemm g2{m, CW * n, CW * rk, ws.l2p2.a.p + off, ws.l2p2.c.p + off, nullptr, (int64_t)CW * n, 0, (int64_t)CW * n};
+        tgemm_f64<double, double>(g2, (const double*)ws.ybuf.p, op.tg_l2p2.p, (double*)ws.eq.p, s);
         ws.launches += 2;
       }
     }
@@ -2965,15 +2836,10 @@ struct Engine {
       const int blocks = nblk(t.n_eval_leafs, EVAL_WARPS);
       NearArgs na{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.n_eval_leafs, t.sbeg.p, t.tbeg.p,
                   t.p2p_off.p,    t.p2p.p,   t.center.p,  t.src4.p,  t.trg4.p,       t.src_qim.p, ws.out.p,
-                  f.k_re,         f.k_im,    ws.srcf.p,   t.x0[0],   t.x0[1],        t.x0[2]};
-      if constexpr (KER == K_LAPLACE && sizeof(R) == 4) {
-        if (t.nsrc > 0) {
-          k_src_split<<<nblk(t.nsrc, 256), 256, 0, s>>>(t.src4.p, t.nsrc, t.x0[0], t.x0[1], t.x0[2], ws.srcf.p);
-          XLAUNCH();
-          ws.launches++;
-        }
+                  f.k_re,         f.k_im};
+      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
         k_near_lap_f2<<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
-      } else
+      else
         k_near<KER, R><<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
       XLAUNCH();
       ws.launches++;
@@ -3093,6 +2959,19 @@ void selftest_bounded_wait(int64_t limit_cycles) {
   int h = 0;
   XCUDA(cudaMemcpy(&h, status.p, sizeof(int), cudaMemcpyDeviceToHost));
   XREQUIRE(!h, XFMM_ERR_TIMEOUT, "bounded device-side wait ran out (self-test)");
+}
+
+// After the caller's stream has been synchronised: XFMM_ERR_TIMEOUT when a bounded device-side wait of the
+// last pass ran out (the flag is cleared for the next pass).
+void check_device_status(Fmm& f, Tree& t) {
+  Workspace* ws = t.ws[f.precision];
+  if (!ws) return;
+  int dev_status = 0;
+  XCUDA(cudaMemcpy(&dev_status, ws->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (dev_status) {
+    XCUDA(cudaMemset(ws->status.p, 0, sizeof(int)));
+    XREQUIRE(false, XFMM_ERR_TIMEOUT, "a bounded device-side wait ran out in the last pass (results incomplete)");
+  }
 }
 
 void stage_times(Fmm& f, Tree& t, double* ms14) {

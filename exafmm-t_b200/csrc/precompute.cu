@@ -17,6 +17,7 @@
 
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <map>
 #include <tuple>
 
@@ -178,12 +179,13 @@ __global__ void k_sinv(const double* s, int n, double thr, double* sinv) {
   if (i < n) sinv[i] = s[i] > thr ? 1.0 / s[i] : 0.0;
 }
 
-// Row-major factors of M = U_M S VH_M from cuSOLVER's column-major SVD of A = M^T = U_c S V_c^H:
-// M = conj(V_c) S U_c^T, and read as row-major arrays the memory of cuSOLVER's U is U_c^T = VH_M
-// and the memory of its VT (= V_c^H, column-major) is conj(V_c) = U_M.
-// Writes the GEMM operands of P2M / L2P and the two factors used to form M2M.
-__global__ void k_svd_factors(const double* Uc, const double* Vc, const double* sinv, int n, int cplx, double* p2m1,
-                              double* p2m2, double* l2p1, double* l2p2, double* Uh, double* Vs) {
+// The reference's four check-to-equivalent factors, row-major n x n (fmm_scale_invariant.h:474-479 real,
+// 505-512 complex) from cuSOLVER's column-major SVD of A = M^T, M = U_M S VH_M the row-major kernel
+// matrix: M = conj(V_c) S U_c^T, so read as row-major arrays the memory of cuSOLVER's U is U_c^T = VH_M and
+// the memory of its VT (= V_c^H, column-major) is conj(V_c) = U_M.  UC2E_U = U^H,
+// UC2E_V = V S+, DC2E_U = conj(VH), DC2E_V = conj(U) S+ (real kernels: no conjugates).
+__global__ void k_ref_factors(const double* Uc, const double* Vc, const double* sinv, int n, int cplx, double* uc2e_u,
+                              double* uc2e_v, double* dc2e_u, double* dc2e_v) {
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= (int64_t)n * n) return;
   const int k = (int)(e / n), j = (int)(e % n);
@@ -192,21 +194,36 @@ __global__ void k_svd_factors(const double* Uc, const double* Vc, const double* 
   if (cplx) {
     const double2* U2 = (const double2*)Uc;
     const double2* V2 = (const double2*)Vc;
-    const double2 vkj = V2[kj], vjk = V2[jk], ukj = U2[kj], ujk = U2[jk];
-    ((double2*)p2m1)[kj] = make_double2(vkj.x, -vkj.y);                      // conj(U_M[k][j])
-    ((double2*)p2m2)[kj] = make_double2(ukj.x * sinv[k], -ukj.y * sinv[k]);  // conj(VH_M[k][j]) / s_k
-    ((double2*)l2p1)[kj] = make_double2(ujk.x, -ujk.y);                      // conj(VH_M[j][k])
-    ((double2*)l2p2)[kj] = make_double2(vjk.x * sinv[k], -vjk.y * sinv[k]);  // conj(U_M[j][k]) / s_k
-    ((double2*)Uh)[kj] = make_double2(vjk.x, -vjk.y);                        // (U_M^H)[k][j] = conj(U_M[j][k])
-    ((double2*)Vs)[kj] = make_double2(ujk.x * sinv[j], -ujk.y * sinv[j]);   // (V_M S+)[k][j]
+    const double2 vjk = V2[jk], ukj = U2[kj], vkj = V2[kj], ujk = U2[jk];
+    ((double2*)uc2e_u)[kj] = make_double2(vjk.x, -vjk.y);                    // conj(U_M[j][k])
+    ((double2*)uc2e_v)[kj] = make_double2(ujk.x * sinv[j], -ujk.y * sinv[j]);  // conj(VH_M[j][k]) / s_j
+    ((double2*)dc2e_u)[kj] = make_double2(ukj.x, -ukj.y);                    // conj(VH_M[k][j])
+    ((double2*)dc2e_v)[kj] = make_double2(vkj.x * sinv[j], -vkj.y * sinv[j]);  // conj(U_M[k][j]) / s_j
   } else {
-    p2m1[kj] = Vc[kj];
-    p2m2[kj] = Uc[kj] * sinv[k];
-    l2p1[kj] = Uc[jk];
-    l2p2[kj] = Vc[jk] * sinv[k];
-    Uh[kj] = Vc[jk];
-    Vs[kj] = Uc[jk] * sinv[j];
+    uc2e_u[kj] = Vc[jk];
+    uc2e_v[kj] = Uc[jk] * sinv[j];
+    dc2e_u[kj] = Uc[kj];
+    dc2e_v[kj] = Vc[kj] * sinv[j];
   }
+}
+
+// out[k][j] = keep(k) ? in[j][k] : 0 (n x n, complex as pairs): the GEMM form of a reference factor, with
+// the columns of dropped singular directions zeroed (keep: the first `rank` columns; rank = n keeps all)
+__global__ void k_factor_T(const double* in, int n, int cplx, int rank, double* out) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n * n) return;
+  const int k = (int)(e / n), j = (int)(e % n);
+  const int64_t src = (int64_t)j * n + k;
+  const bool keep = k < rank;
+  if (cplx) ((double2*)out)[e] = keep ? ((const double2*)in)[src] : make_double2(0, 0);
+  else out[e] = keep ? in[src] : 0.0;
+}
+// columns >= rank of a row-major n x n reference factor set to zero (in place)
+__global__ void k_zero_cols(double* a, int n, int cplx, int rank) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n * n || (int)(e % n) < rank) return;
+  if (cplx) ((double2*)a)[e] = make_double2(0, 0);
+  else a[e] = 0.0;
 }
 
 // T[ipos][f][j] = helper[imap[ipos][j]][f] / nconv
@@ -247,6 +264,73 @@ __global__ void k_to_single(const double* in, float* out, int64_t n) {
 
 inline int nb(int64_t n) { return (int)std::max<int64_t>(1, (n + 255) / 256); }
 
+// ---- the reference's operator file (.dat; fmm_scale_invariant.h:86-148, fmm.h:83-138), FP64 build:
+//   r0 (8 bytes), then per level (Laplace: level 0 only; the other kernels: levels 0..depth)
+//   UC2E_U, UC2E_V, DC2E_U, DC2E_V, M2M[8], L2L[8] (n x n row-major, real or complex values),
+//   then the M2L tables of the table levels (Laplace: one; the others: levels 1..depth), 26 per level,
+//   each [nfreq][8 x 8][re, im] in doubles.  A file is used only when its size and r0 match, as the
+//   reference's load_matrix decides (else the operators are computed and the file rewritten).
+struct DatOps {
+  std::vector<std::array<std::vector<double>, 4>> fac;
+  std::vector<std::vector<double>> m2m, l2l, m2l;
+  void alloc(const Fmm& f, int depth) {
+    const int nlev = f.kernel == XFMM_LAPLACE ? 1 : depth + 1;
+    const int ntab = f.kernel == XFMM_LAPLACE ? 1 : depth;
+    fac.assign(nlev, {});
+    m2m.assign(nlev, {});
+    l2l.assign(nlev, {});
+    m2l.assign(ntab, {});
+  }
+};
+
+size_t dat_bytes(const Fmm& f, int depth) {
+  const size_t vs = f.is_complex() ? 2 : 1, n = f.nsurf;
+  const size_t nlev = f.kernel == XFMM_LAPLACE ? 1 : depth + 1, ntab = f.kernel == XFMM_LAPLACE ? 1 : depth;
+  return sizeof(double) + nlev * 20 * n * n * vs * sizeof(double) + ntab * 26 * (size_t)f.nfreq * 128 * sizeof(double);
+}
+
+bool dat_load(const Fmm& f, int depth, DatOps& d) {
+  FILE* fp = std::fopen(f.filename.c_str(), "rb");
+  if (!fp) return false;
+  std::fseek(fp, 0, SEEK_END);
+  const long size = std::ftell(fp);
+  std::fseek(fp, 0, SEEK_SET);
+  double r0 = 0;
+  bool ok = size >= 0 && (size_t)size == dat_bytes(f, depth) && std::fread(&r0, sizeof(double), 1, fp) == 1 &&
+            r0 == f.r0;
+  if (ok) {
+    d.alloc(f, depth);
+    const size_t vs = f.is_complex() ? 2 : 1, nn = (size_t)f.nsurf * f.nsurf * vs;
+    auto rd = [&](std::vector<double>& v, size_t cnt) {
+      v.resize(cnt);
+      return std::fread(v.data(), sizeof(double), cnt, fp) == cnt;
+    };
+    for (size_t l = 0; ok && l < d.fac.size(); l++) {
+      for (int i = 0; i < 4; i++) ok = ok && rd(d.fac[l][i], nn);
+      ok = ok && rd(d.m2m[l], 8 * nn) && rd(d.l2l[l], 8 * nn);
+    }
+    for (size_t t = 0; ok && t < d.m2l.size(); t++) ok = rd(d.m2l[t], 26 * (size_t)f.nfreq * 128);
+  }
+  std::fclose(fp);
+  return ok;
+}
+
+void dat_save(const Fmm& f, int depth, const DatOps& d) {
+  (void)depth;
+  std::remove(f.filename.c_str());
+  FILE* fp = std::fopen(f.filename.c_str(), "wb");
+  XREQUIRE(fp, XFMM_ERR_ARG, "cannot write the operator file " + f.filename);
+  bool ok = std::fwrite(&f.r0, sizeof(double), 1, fp) == 1;
+  auto wr = [&](const std::vector<double>& v) { return std::fwrite(v.data(), sizeof(double), v.size(), fp) == v.size(); };
+  for (size_t l = 0; ok && l < d.fac.size(); l++) {
+    for (int i = 0; i < 4; i++) ok = ok && wr(d.fac[l][i]);
+    ok = ok && wr(d.m2m[l]) && wr(d.l2l[l]);
+  }
+  for (size_t t = 0; ok && t < d.m2l.size(); t++) ok = wr(d.m2l[t]);
+  ok = (std::fclose(fp) == 0) && ok;
+  XREQUIRE(ok, XFMM_ERR_ARG, "writing the operator file " + f.filename + " failed");
+}
+
 struct Handles {
   cublasHandle_t blas = nullptr;
   cusolverDnHandle_t sol = nullptr;
@@ -255,6 +339,47 @@ struct Handles {
     if (sol) cusolverDnDestroy(sol);
   }
 };
+
+// Row-major complex or real GEMM C = op(P) Q for n x n matrices (op: identity or transpose, never
+// conjugate), on cuBLAS's column-major convention: row-major X is column-major X^T.
+void gemm_rm(cublasHandle_t h, int n, bool cplx, const double* P, bool transP, const double* Q, double* C) {
+  const cublasOperation_t tp = transP ? CUBLAS_OP_T : CUBLAS_OP_N;
+  if (cplx) {
+    const cuDoubleComplex one = make_cuDoubleComplex(1, 0), z = make_cuDoubleComplex(0, 0);
+    XCUBLAS(cublasZgemm(h, CUBLAS_OP_N, tp, n, n, n, &one, (const cuDoubleComplex*)Q, n, (const cuDoubleComplex*)P, n,
+                        &z, (cuDoubleComplex*)C, n));
+  } else {
+    const double one = 1, z = 0;
+    XCUBLAS(cublasDgemm(h, CUBLAS_OP_N, tp, n, n, n, &one, Q, n, P, n, &z, C, n));
+  }
+}
+
+// M2M[c] = UC2E_V (UC2E_U K_c) and, when l2l is given, L2L[c] = (K_c^T DC2E_V) DC2E_U for the 8 children
+// (fmm_scale_invariant.h:51-77, fmm.h:47-74), K_c = K(parent check surface, child c's equivalent surface),
+// each n x n row-major at c n^2 of the outputs.
+void m2m_products(const Fmm& f, cublasHandle_t blas, int lev, const DBuf<double>& d_chk, DBuf<double>& d_eqv,
+                  const DBuf<double>& uc2e_u, const DBuf<double>& uc2e_v, const DBuf<double>& dc2e_u,
+                  const DBuf<double>& dc2e_v, DBuf<double>& K, DBuf<double>& Tmp, double* m2m, double* l2l,
+                  cudaStream_t s) {
+  const int p = f.p, n = f.nsurf;
+  const bool cplx = f.is_complex();
+  const size_t nn = (size_t)n * n * (cplx ? 2 : 1);
+  const auto rel = rel_coords(1, 1, 2);
+  const double sc = f.r0 * std::pow(0.5, lev + 1);
+  for (int c = 0; c < 8; c++) {
+    const double cc[3] = {rel[c][0] * sc, rel[c][1] * sc, rel[c][2] * sc};
+    std::vector<double> ceq = host_surface(p, f.r0, lev + 1, cc, 1.05);
+    d_eqv.upload(ceq, s);
+    k_kernel_matrix<<<nb((int64_t)n * n), 256, 0, s>>>(f.kernel, f.k_re, f.k_im, d_chk.p, n, d_eqv.p, n, K.p, cplx);
+    XLAUNCH();
+    gemm_rm(blas, n, cplx, uc2e_u.p, false, K.p, Tmp.p);
+    gemm_rm(blas, n, cplx, uc2e_v.p, false, Tmp.p, m2m + (size_t)c * nn);
+    if (l2l) {
+      gemm_rm(blas, n, cplx, K.p, true, dc2e_v.p, Tmp.p);
+      gemm_rm(blas, n, cplx, Tmp.p, false, dc2e_u.p, l2l + (size_t)c * nn);
+    }
+  }
+}
 
 }  // namespace
 
@@ -299,79 +424,106 @@ void precompute(Fmm& f, int depth, cudaStream_t s) {
   DBuf<int> d_imap;
   d_imap.upload(imap, s);
   auto helper_rel = rel_coords(3, 2, 1);
-  auto m2m_rel = rel_coords(1, 1, 2);
 
   const int nlev = f.kernel == XFMM_LAPLACE ? 1 : depth + 1;
+  const std::vector<int> tab_levels = f.kernel == XFMM_LAPLACE ? std::vector<int>{0} : [&] {
+    std::vector<int> v;
+    for (int l = 1; l <= depth; l++) v.push_back(l);
+    return v;
+  }();
+  // The reference's FP64 operators (its threshold, its row-major layouts): read from the operator file
+  // when it holds this configuration, else computed here and, when a file is named, written to it.
+  // The working operators of this precision are derived from them below.
+  DatOps dat;
+  const bool named = !f.filename.empty();
+  const bool loaded = named && dat_load(f, depth, dat);
+  if (!loaded) dat.alloc(f, depth);
   f.ops.clear();
   f.ops.resize(nlev);
   const double zero[3] = {0, 0, 0};
-  DBuf<double> d_chk, d_eqv, M(n * (size_t)n * vs), Mcopy(n * (size_t)n * vs), S(n), U(n * (size_t)n * vs),
-      VT(n * (size_t)n * vs), K(n * (size_t)n * vs), M2M(8 * (size_t)n * n * vs), Uh(n * (size_t)n * vs),
-      Vs(n * (size_t)n * vs), Tmp(n * (size_t)n * vs), sinv(n);
-  DBuf<double> F[4];
-  for (auto& b : F) b.alloc(n * (size_t)n * vs);
+  const size_t nn = (size_t)n * n * vs;
+  DBuf<double> d_chk, d_eqv, M(nn), S(n), U(nn), VT(nn), K(nn), Tmp(nn), sinv(n);
+  DBuf<double> R[4], F[4], M2Mref(8 * nn), L2Lref(8 * nn), M2M(8 * nn);
+  for (auto& b : R) b.alloc(nn);
+  for (auto& b : F) b.alloc(nn);
   DBuf<int> info(1);
   for (int lev = 0; lev < nlev; lev++) {
     LevelOps& op = f.ops[lev];
-    // ---- K(check, equiv) and its regularised pinv
-    std::vector<double> chk = host_surface(p, r0, lev, zero, 2.95), eqv = host_surface(p, r0, lev, zero, 1.05);
+    std::vector<double> chk = host_surface(p, r0, lev, zero, 2.95);
     d_chk.upload(chk, s);
-    d_eqv.upload(eqv, s);
-    k_kernel_matrix<<<nb((int64_t)n * n), 256, 0, s>>>(f.kernel, f.k_re, f.k_im, d_chk.p, n, d_eqv.p, n, M.p, cplx);
-    XLAUNCH();
-    XCUDA(cudaMemcpyAsync(Mcopy.p, M.p, M.bytes(), cudaMemcpyDeviceToDevice, s));
-    int lwork = 0;
-    if (cplx) XCUSOLVER(cusolverDnZgesvd_bufferSize(H.sol, n, n, &lwork));
-    else XCUSOLVER(cusolverDnDgesvd_bufferSize(H.sol, n, n, &lwork));
-    DBuf<double> work((size_t)std::max(lwork, 1) * vs), rwork(5 * (size_t)n);
-    if (cplx)
-      XCUSOLVER(cusolverDnZgesvd(H.sol, 'A', 'A', n, n, (cuDoubleComplex*)Mcopy.p, n, S.p, (cuDoubleComplex*)U.p, n,
-                                 (cuDoubleComplex*)VT.p, n, (cuDoubleComplex*)work.p, lwork, rwork.p, info.p));
-    else
-      XCUSOLVER(cusolverDnDgesvd(H.sol, 'A', 'A', n, n, Mcopy.p, n, S.p, U.p, n, VT.p, n, work.p, lwork, rwork.p,
-                                 info.p));
-    int hinfo = 0;
-    XCUDA(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    std::vector<double> hs = S.download(s);
-    XREQUIRE(hinfo == 0, XFMM_ERR_NUMERIC, "check-to-equivalent SVD did not converge");
-    double smax = 0;
-    for (double v : hs) smax = std::max(smax, std::fabs(v));
-    // singular values come in descending order: the factors' first `rank` rows/columns carry everything
-    int rank = 0;
-    for (double v : hs) rank += v > eps * smax * 4;
-    op.rank = std::max(rank, 1);
-    k_sinv<<<nb(n), 256, 0, s>>>(S.p, n, eps * smax * 4, sinv.p);
-    k_svd_factors<<<nb((int64_t)n * n), 256, 0, s>>>(U.p, VT.p, sinv.p, n, cplx, F[0].p, F[1].p, F[2].p, F[3].p,
-                                                      Uh.p, Vs.p);
-    XLAUNCH();
-    // ---- M2M[c] = (V S+) (U^H K(parent check, child equiv)), row-major, in the reference's factored
-    //      order (fmm_scale_invariant.h:67-71); cuBLAS is column-major, so row-major X*Y = gemm(Y, X)
-    const double sc = r0 * std::pow(0.5, lev + 1);
-    for (int c = 0; c < 8; c++) {
-      const double cc[3] = {m2m_rel[c][0] * sc, m2m_rel[c][1] * sc, m2m_rel[c][2] * sc};
-      std::vector<double> ceq = host_surface(p, r0, lev + 1, cc, 1.05);
-      d_eqv.upload(ceq, s);
-      k_kernel_matrix<<<nb((int64_t)n * n), 256, 0, s>>>(f.kernel, f.k_re, f.k_im, d_chk.p, n, d_eqv.p, n, K.p, cplx);
+    if (loaded) {
+      for (int i = 0; i < 4; i++) R[i].upload(dat.fac[lev][i], s);
+      M2Mref.upload(dat.m2m[lev], s);
+      L2Lref.upload(dat.l2l[lev], s);
+    } else {
+      // ---- K(check, equiv), its SVD and the reference's factors at its threshold 4e-16 s_max
+      std::vector<double> eqv = host_surface(p, r0, lev, zero, 1.05);
+      d_eqv.upload(eqv, s);
+      k_kernel_matrix<<<nb((int64_t)n * n), 256, 0, s>>>(f.kernel, f.k_re, f.k_im, d_chk.p, n, d_eqv.p, n, M.p, cplx);
       XLAUNCH();
-      double* out = M2M.p + (size_t)c * n * n * vs;
-      if (cplx) {
-        const cuDoubleComplex one = make_cuDoubleComplex(1, 0), z = make_cuDoubleComplex(0, 0);
-        XCUBLAS(cublasZgemm(H.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, (cuDoubleComplex*)K.p, n,
-                            (cuDoubleComplex*)Uh.p, n, &z, (cuDoubleComplex*)Tmp.p, n));
-        XCUBLAS(cublasZgemm(H.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, (cuDoubleComplex*)Tmp.p, n,
-                            (cuDoubleComplex*)Vs.p, n, &z, (cuDoubleComplex*)out, n));
-      } else {
-        const double one = 1, z = 0;
-        XCUBLAS(cublasDgemm(H.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, K.p, n, Uh.p, n, &z, Tmp.p, n));
-        XCUBLAS(cublasDgemm(H.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Tmp.p, n, Vs.p, n, &z, out, n));
+      int lwork = 0;
+      if (cplx) XCUSOLVER(cusolverDnZgesvd_bufferSize(H.sol, n, n, &lwork));
+      else XCUSOLVER(cusolverDnDgesvd_bufferSize(H.sol, n, n, &lwork));
+      DBuf<double> work((size_t)std::max(lwork, 1) * vs), rwork(5 * (size_t)n);
+      if (cplx)
+        XCUSOLVER(cusolverDnZgesvd(H.sol, 'A', 'A', n, n, (cuDoubleComplex*)M.p, n, S.p, (cuDoubleComplex*)U.p, n,
+                                   (cuDoubleComplex*)VT.p, n, (cuDoubleComplex*)work.p, lwork, rwork.p, info.p));
+      else
+        XCUSOLVER(cusolverDnDgesvd(H.sol, 'A', 'A', n, n, M.p, n, S.p, U.p, n, VT.p, n, work.p, lwork, rwork.p,
+                                   info.p));
+      int hinfo = 0;
+      XCUDA(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      std::vector<double> hs = S.download(s);
+      XREQUIRE(hinfo == 0, XFMM_ERR_NUMERIC, "check-to-equivalent SVD did not converge");
+      double smax = 0;
+      for (double v : hs) smax = std::max(smax, std::fabs(v));
+      k_sinv<<<nb(n), 256, 0, s>>>(S.p, n, 1e-16 * smax * 4, sinv.p);
+      k_ref_factors<<<nb((int64_t)n * n), 256, 0, s>>>(U.p, VT.p, sinv.p, n, cplx, R[0].p, R[1].p, R[2].p, R[3].p);
+      XLAUNCH();
+      // M2M[c] = UC2E_V (UC2E_U K(parent check, child equiv)) (fmm_scale_invariant.h:67-71), L2L[c] =
+      // K^T DC2E_V DC2E_U (72-74), each n x n row-major
+      m2m_products(f, H.blas, lev, d_chk, d_eqv, R[0], R[1], R[2], R[3], K, Tmp, M2Mref.p, L2Lref.p, s);
+      if (named) {
+        for (int i = 0; i < 4; i++) dat.fac[lev][i] = R[i].download(s);
+        dat.m2m[lev] = M2Mref.download(s);
+        dat.l2l[lev] = L2Lref.download(s);
       }
     }
-    // ---- GEMM operands in the working precision
-    // the check-to-equivalent factors stay FP64 in both precisions
+    // ---- the working operators of this precision.  Singular directions kept: those with s_k above
+    // 4 eps s_max, s_k = 1 / |column k of UC2E_V| (V has unit columns; dropped columns are zero).
+    std::vector<double> hv = R[1].download(s);
+    std::vector<double> sk(n, 0.0);
+    double smax = 0;
+    for (int k = 0; k < n; k++) {
+      double c2 = 0;
+      for (int j = 0; j < n; j++)
+        for (int q = 0; q < vs; q++) c2 += hv[((size_t)j * n + k) * vs + q] * hv[((size_t)j * n + k) * vs + q];
+      sk[k] = c2 > 0 ? 1.0 / std::sqrt(c2) : 0.0;
+      smax = std::max(smax, sk[k]);
+    }
+    int rank = 0;  // singular values come in descending order: the kept directions are a prefix
+    while (rank < n && sk[rank] > 0 && (!single || sk[rank] > 4 * eps * smax)) rank++;
+    op.rank = std::max(rank, 1);
+    for (int i = 0; i < 4; i++) {
+      k_factor_T<<<nb((int64_t)n * n), 256, 0, s>>>(R[i].p, n, cplx, (i == 1 || i == 3) ? op.rank : n, F[i].p);
+      XLAUNCH();
+    }
+    const double* m2m_w = M2Mref.p;  // FP64: the reference's M2M, L2L
+    const double* l2l_w = L2Lref.p;
+    if (single) {
+      // mixed: M2M from the factors truncated at the mixed threshold (L2L = its transpose)
+      k_zero_cols<<<nb((int64_t)n * n), 256, 0, s>>>(R[1].p, n, cplx, op.rank);
+      k_zero_cols<<<nb((int64_t)n * n), 256, 0, s>>>(R[3].p, n, cplx, op.rank);
+      XLAUNCH();
+      m2m_products(f, H.blas, lev, d_chk, d_eqv, R[0], R[1], R[2], R[3], K, Tmp, M2M.p, nullptr, s);
+      m2m_w = M2M.p;
+      l2l_w = nullptr;
+    }
+    // ---- GEMM operands: the check-to-equivalent factors stay FP64 in both precisions
     DBuf<char>* dst[4] = {&op.p2m_B1, &op.p2m_B2, &op.l2p_B1, &op.l2p_B2};
     for (int i = 0; i < 4; i++) {
-      dst[i]->alloc((size_t)n * n * vs * sizeof(double));
-      XCUDA(cudaMemcpyAsync(dst[i]->p, F[i].p, (size_t)n * n * vs * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      dst[i]->alloc(nn * sizeof(double));
+      XCUDA(cudaMemcpyAsync(dst[i]->p, F[i].p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
     }
     // the mixed path's L2P first factor (an orthogonal rotation of FP32 check values) runs in FP32
     if (single && !cplx) {
@@ -379,47 +531,58 @@ void precompute(Fmm& f, int depth, cudaStream_t s) {
       k_to_single<<<nb((int64_t)n * n), 256, 0, s>>>(F[2].p, (float*)op.l2p_B1f.p, (int64_t)n * n);
       XLAUNCH();
     }
+    // m2m_B[c n + k][j] = M2M[c][j][k];  l2l_B[k][c n + j] = L2L[c][j][k] (= M2M[c][k][j])
     op.m2m_B.alloc((size_t)8 * n * n * wsz);
     op.l2l_B.alloc((size_t)8 * n * n * wsz);
     for (int c = 0; c < 8; c++) {
-      const double* Mc = M2M.p + (size_t)c * n * n * vs;
+      const double* Mc = m2m_w + (size_t)c * nn;
       k_place<<<nb((int64_t)n * n), 256, 0, s>>>(Mc, n, 1, cplx, n, c * n, 0, op.m2m_B.p, single);
-      k_place<<<nb((int64_t)n * n), 256, 0, s>>>(Mc, n, 0, cplx, 8 * n, 0, c * n, op.l2l_B.p, single);
+      if (l2l_w)
+        k_place<<<nb((int64_t)n * n), 256, 0, s>>>(l2l_w + (size_t)c * nn, n, 1, cplx, 8 * n, 0, c * n, op.l2l_B.p,
+                                                   single);
+      else
+        k_place<<<nb((int64_t)n * n), 256, 0, s>>>(Mc, n, 0, cplx, 8 * n, 0, c * n, op.l2l_B.p, single);
     }
     XLAUNCH();
+    prepare_translation_operands(f, op, s);
   }
 
-  // ---- M2L tables
+  // ---- M2L tables [26][nfreq][64] complex (the reference's matrix_M2L layout), FP64 then working precision
   const int nh = (int)helper_rel.size();
-  const std::vector<int> tab_levels = f.kernel == XFMM_LAPLACE ? std::vector<int>{0} : [&] {
-    std::vector<int> v;
-    for (int l = 1; l <= depth; l++) v.push_back(l);
-    return v;
-  }();
   if (!tab_levels.empty()) {
-    DBuf<double> grid((size_t)nh * nconv * vs), spec((size_t)nh * nfreq * 2), T64((size_t)26 * nfreq * 64 * 2);
+    DBuf<double> grid, spec, T64((size_t)26 * nfreq * 64 * 2);
     DBuf<double> offs(3 * (size_t)nh);
-    cufftHandle plan;
-    int dims[3] = {n1, n1, n1};
-    XCUFFT(cufftPlanMany(&plan, 3, dims, nullptr, 1, nconv, nullptr, 1, nfreq, cplx ? CUFFT_Z2Z : CUFFT_D2Z, nh));
-    XCUFFT(cufftSetStream(plan, s));
-    for (int l : tab_levels) {
-      std::vector<double> ho(3 * nh);
-      for (int h = 0; h < nh; h++)
-        for (int d = 0; d < 3; d++)
-          ho[3 * h + d] = l == 0 ? helper_rel[h][d] * (r0 / 0.5) : helper_rel[h][d] * r0 * std::pow(0.5, l - 1);
-      offs.upload(ho, s);
-      const double a = 2 * r0 * std::pow(0.5, l) * 1.05;
-      k_conv_values<<<nb((int64_t)nh * nconv), 256, 0, s>>>(f.kernel, f.k_re, f.k_im, p, a, offs.p, nh, grid.p,
-                                                             cplx);
-      XLAUNCH();
-      if (cplx)
-        XCUFFT(cufftExecZ2Z(plan, (cufftDoubleComplex*)grid.p, (cufftDoubleComplex*)spec.p, CUFFT_FORWARD));
-      else
-        XCUFFT(cufftExecD2Z(plan, grid.p, (cufftDoubleComplex*)spec.p));
-      k_m2l_tables<<<nb(26ll * nfreq * 64), 256, 0, s>>>((double2*)spec.p, nfreq, d_imap.p, (double)nconv,
-                                                          (double2*)T64.p);
-      XLAUNCH();
+    cufftHandle plan = 0;
+    if (!loaded) {
+      grid.alloc((size_t)nh * nconv * vs);
+      spec.alloc((size_t)nh * nfreq * 2);
+      int dims[3] = {n1, n1, n1};
+      XCUFFT(cufftPlanMany(&plan, 3, dims, nullptr, 1, nconv, nullptr, 1, nfreq, cplx ? CUFFT_Z2Z : CUFFT_D2Z, nh));
+      XCUFFT(cufftSetStream(plan, s));
+    }
+    for (size_t ti = 0; ti < tab_levels.size(); ti++) {
+      const int l = tab_levels[ti];
+      if (loaded) {
+        T64.upload(dat.m2l[ti], s);
+      } else {
+        std::vector<double> ho(3 * nh);
+        for (int h = 0; h < nh; h++)
+          for (int d = 0; d < 3; d++)
+            ho[3 * h + d] = l == 0 ? helper_rel[h][d] * (r0 / 0.5) : helper_rel[h][d] * r0 * std::pow(0.5, l - 1);
+        offs.upload(ho, s);
+        const double a = 2 * r0 * std::pow(0.5, l) * 1.05;
+        k_conv_values<<<nb((int64_t)nh * nconv), 256, 0, s>>>(f.kernel, f.k_re, f.k_im, p, a, offs.p, nh, grid.p,
+                                                               cplx);
+        XLAUNCH();
+        if (cplx)
+          XCUFFT(cufftExecZ2Z(plan, (cufftDoubleComplex*)grid.p, (cufftDoubleComplex*)spec.p, CUFFT_FORWARD));
+        else
+          XCUFFT(cufftExecD2Z(plan, grid.p, (cufftDoubleComplex*)spec.p));
+        k_m2l_tables<<<nb(26ll * nfreq * 64), 256, 0, s>>>((double2*)spec.p, nfreq, d_imap.p, (double)nconv,
+                                                            (double2*)T64.p);
+        XLAUNCH();
+        if (named) dat.m2l[ti] = T64.download(s);
+      }
       LevelOps& op = f.ops[l];
       const int64_t cnt = 26ll * nfreq * 64 * 2;
       if (single) {
@@ -432,8 +595,9 @@ void precompute(Fmm& f, int depth, cudaStream_t s) {
       }
     }
     XCUDA(cudaStreamSynchronize(s));
-    cufftDestroy(plan);
+    if (plan) cufftDestroy(plan);
   }
+  if (named && !loaded) dat_save(f, depth, dat);
   XCUDA(cudaStreamSynchronize(s));
   f.precomputed = true;
   f.pre_r0 = r0;

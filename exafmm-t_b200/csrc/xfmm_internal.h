@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -165,6 +166,12 @@ struct LevelOps {
   DBuf<char> l2l_B;    // [n][8n]     B[k][c*n+j] = M2M[c][k][j] (L2L = M2M^T)
   DBuf<char> m2l_T;    // [26][nfreq][64] complex: entry [s*8+t] (fmm_scale_invariant.h:549-551)
   int rank = 0;        // singular values kept by the pinv threshold: B1 columns / B2 rows beyond are zero
+  // the same operators in the form the translation GEMMs (translate.cu) read: real [K][N] row-major, a
+  // complex operator expanded to [2K][2N] (expand_operator); FP64 for the pinv factors and the FP64
+  // path, TF32 head / tail arrays for the mixed path's M2M, L2L and (real kernels) L2P first factor
+  DBuf<double> tg_p2m1, tg_p2m2, tg_l2p1, tg_l2p2, tg_m2m, tg_l2l;
+  DBuf<float> tg_m2m_h, tg_m2m_l, tg_l2l_h, tg_l2l_l, tg_l2p1_h, tg_l2p1_l;  // mixed: transposed [N][ld]
+  int64_t ld_m2m = 0, ld_l2l = 0, ld_l2p1 = 0;
 };
 
 struct Fmm {
@@ -173,6 +180,7 @@ struct Fmm {
   int nsurf = 0, nconv = 0, nfreq = 0, n1 = 0;
   int depth = 0;
   double x0[3] = {0, 0, 0}, r0 = 0;
+  std::string filename;               // operator file in the reference's .dat layout ("" : none)
   bool precomputed = false;
   double pre_r0 = -1;
   int pre_depth = -1;
@@ -202,6 +210,7 @@ void upward_pass(Fmm& fmm, Tree& t, cudaStream_t s);
 void downward_pass(Fmm& fmm, Tree& t, cudaStream_t s);
 void get_values(Fmm& fmm, Tree& t, double* out_dev, cudaStream_t s);
 void stage_times(Fmm& fmm, Tree& t, double* ms14);
+void check_device_status(Fmm& f, Tree& t);
 void selftest_bounded_wait(int64_t limit_cycles);
 void gradient_p2p_raw(int kernel, double k_re, double k_im, int precision, const double* src, int64_t ns,
                       const double* q, const double* trg, int64_t nt, double* out, cudaStream_t s);
@@ -209,6 +218,31 @@ void verify(Fmm& fmm, Tree& t, int sample, double* err2, cudaStream_t s);
 void gradient_p2p_scratch(int kernel, double k_re, double k_im, int precision, const double* src, int64_t ns,
                           const double* q, const double* trg, int64_t nt, double* out, double4* s4, double* qim,
                           double4* t4, cudaStream_t s);
+// translate.cu: level-batched translation GEMMs with fused row gather / scale / scatter.
+// C[coff[r] + j] (=|+=) alpha[r] * sum_k A[aoff[r] + k] * B[k * ldb + j] for r < M, j < N, k < K, on
+// real views of the rows (complex rows as interleaved reals, operators expanded).
+struct TGemm {
+  int M = 0, N = 0, K = 0;
+  const int64_t* aoff = nullptr;
+  const int64_t* coff = nullptr;
+  const double* alpha = nullptr;  // null: 1
+  int64_t ldb = 0;
+  int accumulate = 0;
+  int64_t astep = 0;  // every A offset is a multiple of astep elements (alignment of the A rows)
+  int* status = nullptr;  // device flag set by a tensor-core GEMM whose bounded wait ran out
+};
+template <class TA, class TC>
+void tgemm_f64(const TGemm& g, const TA* A, const double* B, TC* C, cudaStream_t s);
+template <class TC>
+void tgemm_tf32(const TGemm& g, const float* A, const float* Bh, const float* Bl, TC* C, cudaStream_t s);
+template <class TC>
+void tgemm_tc(const TGemm& g, const float* A, const float* Bth, const float* Btl, int64_t ldbt, TC* C,
+              cudaStream_t s);
+void expand_operator_t(const void* B, bool b_single, int K, int N, int64_t ldb, bool cplx, int npad, int64_t ldbt,
+                       float* ohi, float* olo, cudaStream_t s);
+void expand_operator(const void* B, bool b_single, int K, int N, int64_t ldb, bool cplx, double* o64, float* ohi,
+                     float* olo, cudaStream_t s);
+void prepare_translation_operands(const Fmm& f, LevelOps& op, cudaStream_t s);
 // capi.cpp: record the message returned by xfmm_last_error() on this thread
 void set_last_error(const char* msg);
 

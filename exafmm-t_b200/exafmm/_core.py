@@ -72,6 +72,9 @@ class FmmBase:
         _lib.check(_lib.lib().xfmm_fmm_create(_lib.KERNEL_IDS[self.kernel], self.p, self.ncrit, k.real, k.imag,
                                               _lib.PRECISIONS[precision], ctypes.byref(h)))
         self._h = h
+        if filename:
+            # operators read from / written to this file in the reference's .dat layout at setup
+            _lib.check(_lib.lib().xfmm_fmm_set_operator_file(h, str(filename).encode()))
         self.nsurf = 6 * (self.p - 1) ** 2 + 2
         n1 = 2 * self.p
         self.nconv = n1 ** 3

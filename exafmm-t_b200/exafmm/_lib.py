@@ -24,6 +24,7 @@ SIGNATURES = [
     ("xfmm_version", ctypes.c_char_p, []),
     ("xfmm_fmm_create", i32, [i32, i32, i32, f64, f64, i32, ctypes.POINTER(vp)]),
     ("xfmm_fmm_free", i32, [vp]),
+    ("xfmm_fmm_set_operator_file", i32, [vp, ctypes.c_char_p]),
     ("xfmm_fmm_info", i32, [vp, vp, vp]),
     ("xfmm_build_tree", i32, [vp, vp, i64, vp, i64, i32, i32, vp, ctypes.POINTER(vp)]),
     ("xfmm_tree_free", i32, [vp]),

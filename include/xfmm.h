@@ -6,6 +6,8 @@
  * (namespace exafmm_t; file:line citations are relative to the exafmm-t tree):
  *
  *   xfmm_fmm_create      LaplaceFmm(p, ncrit, filename)                 include/laplace.h:15-22
+ *   xfmm_fmm_set_operator_file  the filename argument + save_matrix/load_matrix
+ *                                                                       include/fmm_scale_invariant.h:86-160
  *                        ModifiedHelmholtzFmm(p, ncrit, wavek, filename)include/modified_helmholtz.h:17-25
  *                        HelmholtzFmm(p, ncrit, wavek, filename)        include/helmholtz.h:16-24
  *   xfmm_build_tree      get_bounds + build_tree + balance_tree         include/build_tree.h:20-35, 181-199, 336-359
@@ -74,6 +76,14 @@ const char* xfmm_version(void);
 /* Fmm object: kernel, expansion order p (2..16), ncrit, wavenumber, precision. */
 xfmm_status xfmm_fmm_create(int kernel, int p, int ncrit, double k_re, double k_im, int precision, xfmm_fmm** out);
 xfmm_status xfmm_fmm_free(xfmm_fmm* fmm);
+/* The constructor's filename argument (include/laplace.h:15-22 and twins; fmm_scale_invariant.h:86-160,
+ * fmm.h:83-153): xfmm_precompute reads the operators from this file when its size and r0 match the
+ * current tree, as the reference's load_matrix does, and otherwise computes them and writes the file.
+ * The file holds the reference's FP64 operators in its .dat layout (r0; per level UC2E_U, UC2E_V, DC2E_U,
+ * DC2E_V, M2M[8], L2L[8]; the M2L tables), so files written by the reference's FP64 build and by this
+ * library are interchangeable.  The mixed precision derives its operators from the same FP64 ones.
+ * NULL or "" (the default) keeps the operators in memory only. */
+xfmm_status xfmm_fmm_set_operator_file(xfmm_fmm* fmm, const char* filename);
 /* Public fields of FmmBase (fmm_base.h:13-23): p, nsurf, nconv, nfreq, ncrit, depth, and x0[3], r0. */
 xfmm_status xfmm_fmm_info(const xfmm_fmm* fmm, int64_t* ints6, double* x0r0_4);
 
@@ -93,7 +103,9 @@ xfmm_status xfmm_clear_values(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
 xfmm_status xfmm_upward_pass(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
 xfmm_status xfmm_downward_pass(xfmm_fmm* fmm, xfmm_tree* tree, void* stream);
 xfmm_status xfmm_get_values(xfmm_fmm* fmm, xfmm_tree* tree, double* out, int on_device, void* stream);
-/* clear_values + upward_pass + downward_pass + get_values. */
+/* clear_values + upward_pass + downward_pass + get_values.  With a host output both return
+ * XFMM_ERR_TIMEOUT when a bounded device-side wait of the pass ran out (the results are then
+ * incomplete); with a device output that is reported by xfmm_stage_times. */
 xfmm_status xfmm_evaluate(xfmm_fmm* fmm, xfmm_tree* tree, double* out, int on_device, void* stream);
 
 /* Tree statistics: nnodes, nleafs, nnonleafs, depth, np2p, nm2p, np2l, n_m2l_src,
@@ -126,8 +138,9 @@ enum {
  * an unknown option or a value out of range. */
 xfmm_status xfmm_set_tuning(xfmm_tree* tree, int option, int value);
 
-/* Direct near-field kernel over raw arrays: out (ntrg x 4) += potential and gradient
- * at trg from (src, q).  precision selects the FP64 or FP32 device kernel. */
+/* Direct near-field kernel over raw arrays: out += potential and gradient at trg from (src, q); out is
+ * ntrg x 4 doubles (Laplace, modified Helmholtz) or ntrg x 8 (Helmholtz: 4 interleaved complex values).
+ * precision selects the FP64 or FP32 device kernel. */
 xfmm_status xfmm_gradient_p2p(int kernel, double k_re, double k_im, int precision, const double* src_xyz,
                               int64_t nsrc, const double* q, const double* trg_xyz, int64_t ntrg, double* out,
                               int on_device, void* stream);
@@ -143,7 +156,9 @@ xfmm_status xfmm_gradient_p2p(int kernel, double k_re, double k_im, int precisio
  * is fixed at start-up).  The first call on each device looks the array up (make it before any
  * stream capture begins); sizes beyond XFMM_NOALLOC_SCRATCH_BYTES return XFMM_ERR_ARG; out is
  * accumulated into (start it at zero for the plain result); the scratch needs no initial contents;
- * the call is asynchronous on stream; overlapping calls on one device share the scratch and race. */
+ * the call is asynchronous on stream; overlapping calls on one device share the scratch and race.  The
+ * array's address is looked up once per device and kept: a device reset (cudaDeviceReset) while the
+ * library is loaded is not supported. */
 xfmm_status xfmm_gradient_p2p_noalloc(int kernel, double k_re, double k_im, int precision, const double* src_xyz,
                                       int64_t nsrc, const double* q, const double* trg_xyz, int64_t ntrg,
                                       double* out, void* stream);
