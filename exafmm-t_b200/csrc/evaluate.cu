@@ -559,13 +559,22 @@ __device__ __forceinline__ void near_leaf(const NearArgs& a, int node, int lane,
 // pair's separation is a single FP32 subtraction of two values no larger than the 3 x 3 x 3 leaf
 // neighbourhood (a few leaf radii).  Its error is a few FP32 ulps of that neighbourhood's size, not of
 // the root's.  That is not enough for the closest pairs (the few pairs a few 1e-5 apart dominate the
-// gradient's norm over all targets), so every pair closer than NEAR_CLOSE x the leaf radius is left out
-// of the FP32 sums and computed again in FP64 from the bodies' FP64 coordinates, by the lanes that met
-// one, after the chunk.  Such pairs are rare (about 2% of the chunks at 4M bodies, p = 8, ncrit = 128),
-// and the error left in the FP32 pairs, ~2^-24 x (neighbourhood radius / separation), is then bounded
-// by separations above NEAR_CLOSE x the leaf radius.  Pairs at r == 0 in FP64 are skipped
-// (laplace.h:57).
+// gradient's norm over all targets), so 1/r is taken of max(r^2, d^2), d = NEAR_CLOSE x the leaf
+// radius: a pair closer than d (r == 0 among them) contributes a bounded FP32 value.  Those pairs are
+// found once per tree with the same FP32 arithmetic (k_close_scan) and, after the near field, k_close_fix
+// replaces each one's FP32 contribution with the exact FP64 one (pairs at r == 0 in FP64 contribute
+// nothing, laplace.h:57).  The error left in the FP32 pairs, ~2^-24 x (neighbourhood radius /
+// separation), is then bounded by separations above d.
 constexpr float NEAR_CLOSE = 0.125f;
+// the squared close-pair distance of a leaf of radius r (the same FP32 value in every kernel that tests it)
+__device__ __forceinline__ float near_close2(double r) {
+  const float d = (float)(NEAR_CLOSE * r);
+  return d * d;
+}
+// a source or target relative to the leaf centre, rounded to FP32 (the same in every kernel)
+__device__ __forceinline__ float3 leaf_rel(const double4& v, const double4& cn) {
+  return make_float3((float)(v.x - cn.x), (float)(v.y - cn.y), (float)(v.z - cn.z));
+}
 #ifndef XFMM_NEAR_CH
 #define XFMM_NEAR_CH 64
 #endif
@@ -574,7 +583,6 @@ static_assert(NEAR_CH == 32 || NEAR_CH == 64, "NEAR_CH");
 struct NearSmemF2 {
   // source pair k = sources 2k, 2k+1 relative to the leaf centre: {x, x'}, {y, y'} and {z, z'}, {q, q'}
   float4 pr[NEAR_CH / 2][2];
-  int64_t sidx[NEAR_CH];  // the chunk's sources in src4 (-1: padding)
   int64_t seg_beg[NEAR_SEG];
   int seg_pre[NEAR_SEG + 1];
 };
@@ -593,23 +601,18 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
   const int tl = lane / G2, sub = lane % G2;
   const int npl = NEAR_CH / 2 / G2;  // source pairs per lane per chunk
   const float2 M1 = make_float2(-1.f, -1.f);
-  const float dc2 = (float)(NEAR_CLOSE * cn.w) * (float)(NEAR_CLOSE * cn.w);  // close-pair threshold, squared
+  const float dc2 = near_close2(cn.w);  // close-pair threshold, squared
   for (int t0 = 0; t0 < T; t0 += 32 * TPL) {
     float2 TX[TPL], TY[TPL], TZ[TPL];
     double P[TPL], GX[TPL], GY[TPL], GZ[TPL];
 #pragma unroll
     for (int u = 0; u < TPL; u++) {
       const int t = t0 + tl + 32 * u;
-      float x = 0.f, y = 0.f, z = 0.f;
-      if (t < T) {
-        const double4 v = a.trg4[tb + t];
-        x = (float)(v.x - cn.x);
-        y = (float)(v.y - cn.y);
-        z = (float)(v.z - cn.z);
-      }
-      TX[u] = dup2(x);
-      TY[u] = dup2(y);
-      TZ[u] = dup2(z);
+      float3 tr = make_float3(0.f, 0.f, 0.f);
+      if (t < T) tr = leaf_rel(a.trg4[tb + t], cn);
+      TX[u] = dup2(tr.x);
+      TY[u] = dup2(tr.y);
+      TZ[u] = dup2(tr.z);
       P[u] = GX[u] = GY[u] = GZ[u] = 0.0;
     }
     for (int64_t eb = e0; eb < e1; eb += NEAR_SEG) {
@@ -642,19 +645,17 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
 #pragma unroll
         for (int h = 0; h < NEAR_CH / 32; h++) {
           const int pos = p0 + 32 * h + lane;
-          // zero-charge padding far away: contributes 0 and never counts as close
+          // zero-charge padding far away: contributes 0 and is never close
           float x = 1e18f, y = 1e18f, z = 1e18f, q = 0.f;
-          int64_t si = -1;
           if (pos < total) {
             while (sm.seg_pre[seg + 1] <= pos) seg++;
-            si = sm.seg_beg[seg] + (pos - sm.seg_pre[seg]);
-            const double4 v = a.src4[si];
-            x = (float)(v.x - cn.x);
-            y = (float)(v.y - cn.y);
-            z = (float)(v.z - cn.z);
+            const double4 v = a.src4[sm.seg_beg[seg] + (pos - sm.seg_pre[seg])];
+            const float3 sr = leaf_rel(v, cn);
+            x = sr.x;
+            y = sr.y;
+            z = sr.z;
             q = (float)v.w;
           }
-          sm.sidx[32 * h + lane] = si;
           float* r = reinterpret_cast<float*>(sm.pr[16 * h + (lane >> 1)]) + (lane & 1);  // float2 slot
           r[0] = x;
           r[2] = y;
@@ -665,12 +666,9 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
         float2 p2[TPL], gx2[TPL], gy2[TPL], gz2[TPL];
 #pragma unroll
         for (int u = 0; u < TPL; u++) p2[u] = gx2[u] = gy2[u] = gz2[u] = make_float2(0.f, 0.f);
-        // pairs closer than the threshold (r == 0 among them) are left out here and redone below; bit jj
-        // of `cm` marks the lane's source pair jj as holding one
-        uint32_t cm = 0;
+        // pairs closer than the threshold (r == 0 among them) give 1/max(r, d): replaced exactly later
 #pragma unroll 4
         for (int jj = 0; jj < npl; jj++) {
-          bool cl = false;
           const int jp = jj * G2 + sub;  // source pair
           const float4 A0 = sm.pr[jp][0], A1 = sm.pr[jp][1];
           const float2 SX = make_float2(A0.x, A0.y), SY = make_float2(A0.z, A0.w);
@@ -683,9 +681,7 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
             float2 r2 = __fmul2_rn(dx, dx);
             r2 = __ffma2_rn(dy, dy, r2);
             r2 = __ffma2_rn(dz, dz, r2);
-            const bool fa = r2.x > dc2, fb = r2.y > dc2;
-            cl |= !(fa && fb);
-            const float2 inv = make_float2(fa ? rsqrtf(r2.x) : 0.f, fb ? rsqrtf(r2.y) : 0.f);
+            const float2 inv = make_float2(rsqrtf(fmaxf(r2.x, dc2)), rsqrtf(fmaxf(r2.y, dc2)));
             const float2 qi = __fmul2_rn(Q, inv);
             const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
             p2[u] = __fadd2_rn(p2[u], qi);
@@ -693,7 +689,6 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
             gy2[u] = __ffma2_rn(qi3, dy, gy2[u]);
             gz2[u] = __ffma2_rn(qi3, dz, gz2[u]);
           }
-          if (cl) cm |= 1u << jj;
         }
 #pragma unroll
         for (int u = 0; u < TPL; u++) {
@@ -701,41 +696,6 @@ __device__ __forceinline__ void near_leaf_lap_f2(const NearArgs& a, int node, in
           GX[u] -= (double)(gx2[u].x + gx2[u].y);
           GY[u] -= (double)(gy2[u].x + gy2[u].y);
           GZ[u] -= (double)(gz2[u].x + gz2[u].y);
-        }
-        while (cm) {  // the lane's close pairs, in FP64 (the same FP32 test picks them out)
-          {
-            const int jj = __ffs(cm) - 1;
-            cm &= cm - 1;
-            const int jp = jj * G2 + sub;
-            const float4 A0 = sm.pr[jp][0], A1 = sm.pr[jp][1];
-            const float2 SX = make_float2(A0.x, A0.y), SY = make_float2(A0.z, A0.w);
-            const float2 SZ = make_float2(A1.x, A1.y);
-#pragma unroll
-            for (int u = 0; u < TPL; u++) {
-              const int t = t0 + tl + 32 * u;
-              if (t >= T) continue;
-              const float2 dx = __ffma2_rn(SX, M1, TX[u]);
-              const float2 dy = __ffma2_rn(SY, M1, TY[u]);
-              const float2 dz = __ffma2_rn(SZ, M1, TZ[u]);
-              float2 r2 = __fmul2_rn(dx, dx);
-              r2 = __ffma2_rn(dy, dy, r2);
-              r2 = __ffma2_rn(dz, dz, r2);
-#pragma unroll
-              for (int h = 0; h < 2; h++) {
-                const int64_t si = sm.sidx[2 * jp + h];
-                if ((h == 0 ? r2.x : r2.y) > dc2 || si < 0) continue;
-                const double4 tv = a.trg4[tb + t], sv = a.src4[si];
-                const double ex = tv.x - sv.x, ey = tv.y - sv.y, ez = tv.z - sv.z;
-                const double e2 = ex * ex + ey * ey + ez * ez;
-                if (e2 == 0.0) continue;  // r == 0 contributes nothing (laplace.h:57)
-                const double ir = rsqrt(e2), qi = sv.w * ir, qi3 = qi * ir * ir;
-                P[u] += qi;
-                GX[u] -= qi3 * ex;
-                GY[u] -= qi3 * ey;
-                GZ[u] -= qi3 * ez;
-              }
-            }
-          }
         }
       }
     }
@@ -777,6 +737,100 @@ __global__ void __launch_bounds__(128, XFMM_NEARF2_MINB) k_near_lap_f2(NearArgs 
   if (T <= 32) near_leaf_lap_f2<1>(a, node, lane, sm[wid]);
   else if (T <= 64 || XFMM_NEARF2_TPL == 2) near_leaf_lap_f2<2>(a, node, lane, sm[wid]);
   else near_leaf_lap_f2<XFMM_NEARF2_TPL>(a, node, lane, sm[wid]);
+}
+
+// The near field's close pairs (k_near_lap_f2): every (target, source) of a leaf's U list whose FP32
+// leaf-relative separation, computed exactly as the near-field kernel computes it, is not above the
+// leaf's close-pair distance.  Warp per target leaf; the U-list sources pass through shared memory 32 at
+// a time.  FILL = false counts them (one global counter), FILL = true writes (target position in tree
+// order, source position, leaf node, 0) at positions taken from a second counter.
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_close_scan(NearArgs a, unsigned long long* __restrict__ counter,
+                                                    int4* __restrict__ pairs, int64_t capacity) {
+  __shared__ float4 ss[4][32];
+  __shared__ int sidx[4][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int w = blockIdx.x * 4 + wid;
+  if (w >= a.n_eval) return;
+  const int node = a.leafs[a.eval_leafs[w]];
+  const int T = a.ntrgs[node];
+  const int64_t tb = a.tbeg[node];
+  const double4 cn = a.center[node];
+  const float dc2 = near_close2(cn.w);
+  unsigned long long found = 0;
+  for (int64_t e = a.p2p_off[node]; e < a.p2p_off[node + 1]; e++) {
+    const int sn = a.p2p[e];
+    const int ns = a.nsrcs[sn];
+    const int64_t sb = a.sbeg[sn];
+    for (int j0 = 0; j0 < ns; j0 += 32) {
+      __syncwarp();
+      if (j0 + lane < ns) {
+        const float3 r = leaf_rel(a.src4[sb + j0 + lane], cn);
+        ss[wid][lane] = make_float4(r.x, r.y, r.z, 0.f);
+        sidx[wid][lane] = (int)(sb + j0 + lane);
+      }
+      __syncwarp();
+      const int cnt = min(32, ns - j0);
+      for (int t = lane; t < T; t += 32) {
+        const float3 tr = leaf_rel(a.trg4[tb + t], cn);
+        for (int j = 0; j < cnt; j++) {
+          const float4 sr = ss[wid][j];
+          const float dx = __fmaf_rn(sr.x, -1.f, tr.x), dy = __fmaf_rn(sr.y, -1.f, tr.y),
+                      dz = __fmaf_rn(sr.z, -1.f, tr.z);
+          float r2 = __fmul_rn(dx, dx);
+          r2 = __fmaf_rn(dy, dy, r2);
+          r2 = __fmaf_rn(dz, dz, r2);
+          if (!(r2 > dc2)) {
+            if (FILL) {
+              const unsigned long long k = atomicAdd(counter, 1ull);
+              if ((int64_t)k < capacity) pairs[k] = make_int4((int)(tb + t), sidx[wid][j], node, 0);
+            } else {
+              found++;
+            }
+          }
+        }
+      }
+    }
+  }
+  if (!FILL) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) found += __shfl_xor_sync(0xffffffffu, found, o);
+    if (lane == 0 && found) atomicAdd(counter, found);
+  }
+}
+
+// For each close pair: the exact FP64 contribution (r == 0 skipped, laplace.h:57) in place of the bounded
+// FP32 one that k_near_lap_f2 added (recomputed with the same operations; the gradient's FP32 product is
+// taken exactly in FP64, as the fused multiply-add took it).
+__global__ void k_close_fix(const int4* __restrict__ pairs, int64_t n, NearArgs a) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int4 pr = pairs[k];
+  const double4 tv = a.trg4[pr.x], sv = a.src4[pr.y], cn = a.center[pr.z];
+  const float dc2 = near_close2(cn.w);
+  const float3 tr = leaf_rel(tv, cn), sr = leaf_rel(sv, cn);
+  const float dx = __fmaf_rn(sr.x, -1.f, tr.x), dy = __fmaf_rn(sr.y, -1.f, tr.y), dz = __fmaf_rn(sr.z, -1.f, tr.z);
+  float r2 = __fmul_rn(dx, dx);
+  r2 = __fmaf_rn(dy, dy, r2);
+  r2 = __fmaf_rn(dz, dz, r2);
+  const float inv = rsqrtf(fmaxf(r2, dc2));
+  const float qi = __fmul_rn((float)sv.w, inv);
+  const float qi3 = __fmul_rn(qi, __fmul_rn(inv, inv));
+  double p = -(double)qi, gx = (double)qi3 * dx, gy = (double)qi3 * dy, gz = (double)qi3 * dz;  // remove FP32
+  const double ex = tv.x - sv.x, ey = tv.y - sv.y, ez = tv.z - sv.z;
+  const double e2 = ex * ex + ey * ey + ez * ez;
+  if (e2 > 0.0) {
+    const double ir = rsqrt(e2), qe = sv.w * ir, qe3 = qe * ir * ir;
+    p += qe;
+    gx -= qe3 * ex;
+    gy -= qe3 * ey;
+    gz -= qe3 * ez;
+  }
+  double* o = a.out + (int64_t)pr.x * 4;
+  atomicAdd(o, p * INV4PI);
+  atomicAdd(o + 1, gx * INV4PI);
+  atomicAdd(o + 2, gy * INV4PI);
+  atomicAdd(o + 3, gz * INV4PI);
 }
 
 #ifndef XFMM_NEAR_MAXTPL
@@ -2205,6 +2259,9 @@ struct Workspace {
   int precision = -1, kernel = -1, p = 0;
   size_t vsz = 0;
   DBuf<char> up, dn, chk;  // working precision
+  DBuf<double> tc_scratch;  // FP64 sums of the split-K tensor-core translations (zero between uses)
+  DBuf<int4> close_pairs;   // Laplace mixed near field: the close pairs (k_close_scan), found once per tree
+  int64_t n_close = -1;     // -1: not searched yet
   DBuf<char> ybuf, eq;     // FP64: pinv intermediate (rows of the kept singular directions), downward
                            // equivalent densities of the leaves
   DBuf<double> out;
@@ -2344,6 +2401,19 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
       }
     upload_rows<double>(W.m2m[l], ma, mc, one, s);
     upload_rows<double>(W.l2l[l], la, lc, one, s);
+  }
+  if (f.mixed()) {
+    // FP64 scratch of the split-K tensor-core M2M / L2L of the small levels, zeroed once
+    const int cw = cplx ? 2 : 1;
+    int64_t need = 0;
+    for (int l = 0; l <= t.depth; l++) {
+      need = std::max(need, tgemm_tc_scratch(W.m2m[l].M, cw * n, cw * 8 * n, 1));
+      need = std::max(need, tgemm_tc_scratch(W.l2l[l].M, cw * 8 * n, cw * n, 1));
+    }
+    if (need > 0) {
+      W.tc_scratch.alloc((size_t)need);
+      XCUDA(cudaMemsetAsync(W.tc_scratch.p, 0, W.tc_scratch.bytes(), s));
+    }
   }
   // M2L buffers and FFT plans
   const int ng = (int)t.m2l_src_off.size() - 1;
@@ -2516,6 +2586,27 @@ template <class RB> const RB* m2l_scale_of(const Tree& t);
 template <> const float* m2l_scale_of<float>(const Tree& t) { return t.m2l_scale.p; }
 template <> const double* m2l_scale_of<double>(const Tree& t) { return t.m2l_scale64.p; }
 
+// The near field's close pairs of this tree (count, then fill), once per workspace; no allocation while
+// evaluating afterwards.
+void find_close_pairs(Workspace& ws, const NearArgs& na, int n_eval, cudaStream_t s) {
+  DBuf<unsigned long long> cnt(2);
+  XCUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), s));
+  if (n_eval > 0) {
+    k_close_scan<false><<<nblk(n_eval, 4), 128, 0, s>>>(na, cnt.p, nullptr, 0);
+    XLAUNCH();
+  }
+  unsigned long long n = 0;
+  XCUDA(cudaMemcpyAsync(&n, cnt.p, sizeof(n), cudaMemcpyDeviceToHost, s));
+  XCUDA(cudaStreamSynchronize(s));
+  ws.close_pairs.alloc(std::max<unsigned long long>(n, 1));
+  if (n > 0) {
+    k_close_scan<true><<<nblk(n_eval, 4), 128, 0, s>>>(na, cnt.p + 1, ws.close_pairs.p, (int64_t)n);
+    XLAUNCH();
+    XCUDA(cudaStreamSynchronize(s));  // cnt is released on return
+  }
+  ws.n_close = (int64_t)n;
+}
+
 // ------------------------------------------------------------------ engine, per kernel and precision
 template <int KER, class R>
 struct Engine {
@@ -2565,8 +2656,12 @@ struct Engine {
       const GemmRows& g = ws.m2m[l];
       if (g.M <= 0) continue;
       const LevelOps& op = level_ops(f, l);
-      TGemm gm{g.M, CW * n, CW * 8 * n, g.a.p, g.c.p, nullptr, (int64_t)CW * n, 0, (int64_t)CW * n};
+      // the parents' rows start at zero (clear_values): the products are added to them, as the reference
+      // adds each child's contribution (fmm_scale_invariant.h:243-251)
+      TGemm gm{g.M, CW * n, CW * 8 * n, g.a.p, g.c.p, nullptr, (int64_t)CW * n, 1, (int64_t)CW * n};
       gm.status = ws.status.p;
+      gm.scratch = ws.tc_scratch.p;
+      gm.scratch_len = (int64_t)ws.tc_scratch.n;
       if constexpr (sizeof(R) == 4)
         tgemm_tc<float>(gm, (const float*)ws.up.p, op.tg_m2m_h.p, op.tg_m2m_l.p, op.ld_m2m, (float*)ws.up.p, s);
       else
@@ -2791,6 +2886,8 @@ struct Engine {
       const LevelOps& op = level_ops(f, l);
       TGemm gl{g.M, CW * 8 * n, CW * n, g.a.p, g.c.p, nullptr, (int64_t)CW * 8 * n, 1, (int64_t)CW * n};
       gl.status = ws.status.p;
+      gl.scratch = ws.tc_scratch.p;
+      gl.scratch_len = (int64_t)ws.tc_scratch.n;
       if constexpr (sizeof(R) == 4)
         tgemm_tc<float>(gl, (const float*)ws.dn.p, op.tg_l2l_h.p, op.tg_l2l_l.p, op.ld_l2l, (float*)ws.dn.p, s);
       else
@@ -2837,12 +2934,21 @@ struct Engine {
       NearArgs na{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.n_eval_leafs, t.sbeg.p, t.tbeg.p,
                   t.p2p_off.p,    t.p2p.p,   t.center.p,  t.src4.p,  t.trg4.p,       t.src_qim.p, ws.out.p,
                   f.k_re,         f.k_im};
-      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
+      if constexpr (KER == K_LAPLACE && sizeof(R) == 4) {
+        if (ws.n_close < 0) find_close_pairs(ws, na, t.n_eval_leafs, s);
         k_near_lap_f2<<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
-      else
+        XLAUNCH();
+        ws.launches++;
+        if (ws.n_close > 0) {
+          k_close_fix<<<nblk(ws.n_close, 256), 256, 0, s>>>(ws.close_pairs.p, ws.n_close, na);
+          XLAUNCH();
+          ws.launches++;
+        }
+      } else {
         k_near<KER, R><<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
-      XLAUNCH();
-      ws.launches++;
+        XLAUNCH();
+        ws.launches++;
+      }
       XCUDA(cudaEventRecord(ws.ev[8], s));
       a.do_near = 0;
       a.accumulate = 1;

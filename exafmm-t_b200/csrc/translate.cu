@@ -310,21 +310,29 @@ __global__ void __launch_bounds__(TG_NT, 4) k_tgemm_tf32(int M, int N, int K, co
 }
 
 // ---------------------------------------------------------------- FP32 accuracy on tcgen05 (TF32 x 3)
-// The same C = alpha A B as k_tgemm_tf32 on the sm_100 tensor cores: a CTA owns 128 rows (one per TMEM
-// lane) and 64 columns.  Per 16-wide K step the 4 warps load the rows' A pieces (coalesced, 16 bytes per
-// lane), split them into TF32 head and tail and store both into shared memory as K-major core matrices
-// (8 rows x 16 bytes, 128 contiguous bytes each); the operator's head and tail, pre-split and stored
-// transposed ([N][K], zero-padded to whole tiles), arrive by cp.async in the same layout.  One elected
-// lane of warp 0 issues the step's six MMAs (M128 N64 K8, Ah Bt + At Bh + Ah Bh per half step, the first
-// into a fresh accumulator) into one of two TMEM accumulators and commits them to that accumulator's
-// mbarrier.  While they run, every warp reads the previous step's accumulator back (its 32 lanes x 64
-// columns) and adds it to FP32 running sums with round-to-nearest adds, then stages the next step.
-// Waits are bounded (about a second); one that runs out sets the status flag and ends the loop.
-constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 16, TC_NT = 128;
+// The same C = alpha A B as k_tgemm_tf32 on the sm_100 tensor cores.  A CTA owns 128 rows (one per TMEM
+// lane), 64 columns and a range of 16-wide K steps (K split over blockIdx.z when a level has few rows;
+// the parts are then added into C with atomics, C already holding the rows' starting values).
+// Per step: the rows' A pieces arrive raw by cp.async two steps ahead (16 bytes per lane, coalesced), are
+// split into TF32 head and tail one step ahead and stored into shared memory as K-major core matrices
+// (8 rows x 16 bytes, 128 contiguous bytes each); the operator's head and tail (pre-split, transposed to
+// [N][K], zero-padded to whole tiles) arrive by cp.async in the same layout, two steps ahead.  One
+// elected lane of warp 0 issues the step's six MMAs (M128 N64 K8; Ah Bt + At Bh + Ah Bh per half step,
+// the first into a fresh accumulator) into one of two TMEM accumulators and commits them to that
+// accumulator's mbarrier.  While they run, every warp reads the previous step's accumulator back (its 32
+// lanes x 64 columns) and adds it to FP32 running sums with round-to-nearest adds.  Waits are bounded
+// (about a second); one that runs out sets the status flag and ends the loop.
+constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 16, TC_NT = 128, TC_ST = 3;
+#ifndef XFMM_TC_KSPLIT_MAX
+#define XFMM_TC_KSPLIT_MAX 64  // largest K split of a tensor-core translation GEMM
+#endif
+#ifndef XFMM_TC_KSPLIT_CTAS
+#define XFMM_TC_KSPLIT_CTAS (2 * 2 * 148)  // CTAs a split aims at (two per SM, two waves)
+#endif
 constexpr uint32_t TC_CORE = 128;                                         // bytes per core matrix
 constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK * 4, TC_B_BYTES = TC_BN * TC_BK * 4;
 constexpr uint32_t TC_STAGE = 2 * TC_A_BYTES + 2 * TC_B_BYTES;            // A head, A tail, B head, B tail
-constexpr size_t TC_SMEM = 2 * (size_t)TC_STAGE + 1024;                  // two stages (+ alignment slack)
+constexpr size_t TC_SMEM = TC_ST * (size_t)TC_STAGE + 2 * (size_t)TC_A_BYTES + 1024;  // + 2 raw A buffers, alignment
 constexpr long long TC_WAIT = 2000000000LL;
 
 // byte offset of element (row, k) (k < 16) in a K-major tile of 16-wide rows: core (row / 8, k / 4)
@@ -339,24 +347,42 @@ __device__ __forceinline__ void tc_mma_ss(uint32_t d_tmem, uint64_t a_desc, uint
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// register <- TMEM, shape 32x32b repeated 64 times: lane i of the warp gets 64 consecutive 32-bit columns
+// of TMEM lane (lane field of taddr) + i
+__device__ __forceinline__ void ld_32x32b_x64(uint32_t taddr, uint32_t (&v)[64]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+               : "r"(taddr)
+               : "memory");
+}
+// Waits (spinning) for the phase of the given parity; false after `limit` SM clock cycles
+__device__ __forceinline__ bool mbar_spin(uint32_t mbar, uint32_t parity, long long limit) {
+  if (tc5::mbar_try_wait(mbar, parity)) return true;
+  const long long t0 = clock64();
+  while (!tc5::mbar_try_wait(mbar, parity))
+    if (clock64() - t0 > limit) return false;
+  return true;
+}
 
 template <class TC, int VA>
-__global__ void __launch_bounds__(TC_NT, 4)
+__global__ void __launch_bounds__(TC_NT, 2)
     k_tgemm_tc(int M, int N, int K, const float* __restrict__ A, const int64_t* __restrict__ aoff,
                const float* __restrict__ Bth, const float* __restrict__ Btl, int64_t ldbt,
                const double* __restrict__ alpha, TC* __restrict__ C, const int64_t* __restrict__ coff, int acc,
-               int* __restrict__ status) {
+               int* __restrict__ status, double* __restrict__ scratch) {
   using namespace tc5;
   extern __shared__ __align__(16) unsigned char tc_raw[];
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag;
-  // stage buffers on a 1 KB boundary
-  unsigned char* sm = tc_raw + ((1024 - (smem_u32(tc_raw) & 1023)) & 1023);
+  unsigned char* sm = tc_raw + ((1024 - (smem_u32(tc_raw) & 1023)) & 1023);  // stages on a 1 KB boundary
+  unsigned char* rawA = sm + TC_ST * (size_t)TC_STAGE;                        // 2 raw A buffers
   const uint32_t sm_u = smem_u32(sm);
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
-  const int nc = (K + TC_BK - 1) / TC_BK;
+  // this CTA's K steps
+  const int nsteps = (K + TC_BK - 1) / TC_BK, per = (nsteps + gridDim.z - 1) / gridDim.z;
+  const int c0 = blockIdx.z * per, nc = max(0, min(nsteps, c0 + per) - c0);
   if (w == 0) {
     tmem_alloc(smem_u32(&tmem_base), 128);
     tmem_relinquish();
@@ -371,22 +397,27 @@ __global__ void __launch_bounds__(TC_NT, 4)
   __syncthreads();
   fence_after_sync();
   const uint32_t tm = tmem_base;
-  // A rows of this thread's pieces: piece q = tid + 128 i -> row q / 4, core column q % 4
+  // this thread's A pieces: piece q = tid + 128 i -> row (q % 8) + 8 (q / 32), K elements 4 kc .. 4 kc + 3
+  // of the step, kc = (q / 8) % 4.  A warp reads 8 rows x 64 bytes (coalesced) and every 8-lane phase of
+  // a 16-byte shared-memory access covers one 128-byte core matrix (no bank conflicts).
+  auto prow = [](int q) { return (q & 7) + 8 * (q >> 5); };
   int64_t arow[4];
 #pragma unroll
   for (int i = 0; i < 4; i++) {
-    const int r = m0 + ((tid + TC_NT * i) >> 2);
+    const int r = m0 + prow(tid + TC_NT * i);
     arow[i] = r < M ? aoff[r] : -1;
   }
-  const int kq = (tid & 3) * 4;  // first K element of this thread's pieces
-  auto stage = [&](int c) {
-    unsigned char* st = sm + (size_t)(c & 1) * TC_STAGE;
+  const int kq = ((tid >> 3) & 3) * 4;
+  // raw A pieces (zero-filled outside the rows and K) and the operator rows of step c (absolute index),
+  // one cp.async group
+  auto fetch = [&](int c) {
+    unsigned char* st = sm + (size_t)(c % TC_ST) * TC_STAGE;
+    unsigned char* ra = rawA + (size_t)(c & 1) * TC_A_BYTES;
     const int k0 = c * TC_BK;
-    // operator head / tail rows n0 .. n0 + 63 (transposed, padded: always in bounds)
 #pragma unroll
     for (int i = 0; i < 2; i++) {
-      const int q = tid + TC_NT * i, row = q >> 2, kk = (q & 3) * 4;
-      const int64_t o = (int64_t)(n0 + row) * ldbt + k0 + kk;
+      const int q = tid + TC_NT * i, row = prow(q), kk = ((q >> 3) & 3) * 4;
+      const int64_t o = (int64_t)(n0 + row) * ldbt + k0 + kk;  // padded operator: always in bounds
       const uint32_t d = tc_off(row, kk);
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(st + 2 * TC_A_BYTES + d)), "l"(Bth + o)
                    : "memory");
@@ -394,38 +425,45 @@ __global__ void __launch_bounds__(TC_NT, 4)
                    "l"(Btl + o)
                    : "memory");
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    // A pieces, split into TF32 head and tail
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-      const int row = (tid + TC_NT * i) >> 2;
-      float v[4] = {0.f, 0.f, 0.f, 0.f};
-      if (arow[i] >= 0) {
-        const float* src = A + arow[i] + k0 + kq;
-        if (k0 + kq + 3 < K) {
-          if constexpr (VA == 16) {
-            const float4 x = *reinterpret_cast<const float4*>(src);
-            v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = x.w;
-          } else {
-            const float2 x = *reinterpret_cast<const float2*>(src), y = *reinterpret_cast<const float2*>(src + 2);
-            v[0] = x.x, v[1] = x.y, v[2] = y.x, v[3] = y.y;
-          }
-        } else {
-#pragma unroll
-          for (int e = 0; e < 4; e++)
-            if (k0 + kq + e < K) v[e] = src[e];
-        }
+      const int k = k0 + kq;
+      const int left = K - k;
+      const uint32_t dst = smem_u32(ra + (size_t)(tid + TC_NT * i) * 16);
+      const bool any = arow[i] >= 0 && left > 0;
+      const float* src = any ? A + arow[i] + k : A;  // a chunk that reads nothing still names A
+      if constexpr (VA == 16) {
+        const uint32_t valid = any ? (uint32_t)(left >= 4 ? 16 : 4 * left) : 0u;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid) : "memory");
+      } else {
+        const uint32_t v0 = any ? (uint32_t)(left >= 2 ? 8 : 4 * left) : 0u;
+        const uint32_t v1 = (any && left > 2) ? (uint32_t)(left >= 4 ? 8 : 4 * (left - 2)) : 0u;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(v0) : "memory");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst + 8), "l"(v1 ? src + 2 : A), "r"(v1)
+                     : "memory");
       }
-      uint32_t h[4], l[4];
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // this thread's raw pieces of step c (its own copies) split into the head and tail tiles of its stage
+  auto split = [&](int c) {
+    unsigned char* st = sm + (size_t)(c % TC_ST) * TC_STAGE;
+    const unsigned char* ra = rawA + (size_t)(c & 1) * TC_A_BYTES;
 #pragma unroll
-      for (int e = 0; e < 4; e++) split_tf32(v[e], h[e], l[e]);
-      const uint32_t d = tc_off(row, kq);
+    for (int i = 0; i < 4; i++) {
+      const int q = tid + TC_NT * i;
+      const float4 v = *reinterpret_cast<const float4*>(ra + (size_t)q * 16);
+      uint32_t h[4], l[4];
+      split_tf32(v.x, h[0], l[0]);
+      split_tf32(v.y, h[1], l[1]);
+      split_tf32(v.z, h[2], l[2]);
+      split_tf32(v.w, h[3], l[3]);
+      const uint32_t d = tc_off(prow(q), kq);
       *reinterpret_cast<uint4*>(st + d) = make_uint4(h[0], h[1], h[2], h[3]);
       *reinterpret_cast<uint4*>(st + TC_A_BYTES + d) = make_uint4(l[0], l[1], l[2], l[3]);
     }
   };
-  auto publish = [&]() {  // this thread's staged data visible to the tensor core, then a CTA barrier
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
+  auto barrier = [&]() {  // shared-memory writes visible to the tensor core, then a CTA barrier
     fence_proxy_async_smem();
     fence_before_sync();
     __syncthreads();
@@ -434,30 +472,32 @@ __global__ void __launch_bounds__(TC_NT, 4)
   float run[TC_BN];
 #pragma unroll
   for (int j = 0; j < TC_BN; j++) run[j] = 0.f;
-  auto readout = [&](int buf) {
-    const uint32_t base = tm + ((uint32_t)(32 * w) << 16) + (uint32_t)(64 * buf);
+  auto readout = [&](int buf) {  // the warp's 32 lanes x 64 columns in one load, one wait
+    uint32_t v[TC_BN];
+    ld_32x32b_x64(tm + ((uint32_t)(32 * w) << 16) + (uint32_t)(64 * buf), v);
+    wait_ld();
 #pragma unroll
-    for (int j = 0; j < TC_BN; j += 16) {
-      uint32_t v[16];
-      ld_32x32b_x16(base + j, v);
-      wait_ld();
-#pragma unroll
-      for (int e = 0; e < 16; e++) run[j + e] = __fadd_rn(run[j + e], __uint_as_float(v[e]));
-    }
+    for (int j = 0; j < TC_BN; j++) run[j] = __fadd_rn(run[j], __uint_as_float(v[j]));
   };
   constexpr uint32_t IDESC = idesc_tf32(TC_BM, TC_BN);
+  // prologue: steps 0 and 1 fetched, step 0 split
+  if (nc > 0) fetch(c0);
+  if (nc > 1) fetch(c0 + 1);
+  if (nc > 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
+  else asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (nc > 0) split(c0);
+  barrier();
   bool ok = true;
-  if (nc > 0) stage(0);
-  publish();
-  for (int c = 0; c < nc && ok; c++) {
-    const int s = c & 1;
+  for (int i = 0; i < nc && ok; i++) {
+    const int c = c0 + i, s = i & 1;
     if (w == 0) {
       if (elect_one()) {
-        const uint32_t st = sm_u + (uint32_t)s * TC_STAGE;
+        const uint32_t st = sm_u + (uint32_t)(c % TC_ST) * TC_STAGE;
 #pragma unroll
         for (int ks = 0; ks < 2; ks++) {  // half steps K 8 ks .. 8 ks + 7: core columns 2 ks, 2 ks + 1
           const uint32_t o = 2 * ks * TC_CORE;
-          const uint64_t ah = sdesc_nosw(st + o, TC_CORE, 4 * TC_CORE), al = sdesc_nosw(st + TC_A_BYTES + o, TC_CORE, 4 * TC_CORE);
+          const uint64_t ah = sdesc_nosw(st + o, TC_CORE, 4 * TC_CORE),
+                         al = sdesc_nosw(st + TC_A_BYTES + o, TC_CORE, 4 * TC_CORE);
           const uint64_t bh = sdesc_nosw(st + 2 * TC_A_BYTES + o, TC_CORE, 4 * TC_CORE),
                          bl = sdesc_nosw(st + 2 * TC_A_BYTES + TC_B_BYTES + o, TC_CORE, 4 * TC_CORE);
           const uint32_t d = tm + 64 * s;
@@ -469,46 +509,73 @@ __global__ void __launch_bounds__(TC_NT, 4)
       }
       __syncwarp();
     }
-    if (c >= 1) {
-      // the previous step's MMAs (accumulator and stage s ^ 1) are complete: read it back, then restage
-      ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&mbar[s ^ 1]), ((c - 1) >> 1) & 1, TC_WAIT));
-      if (ok) {
+    if (i >= 1) {
+      // the previous step's MMAs are complete: its accumulator is read back, its stage is free
+      if (__all_sync(0xffffffffu, mbar_spin(smem_u32(&mbar[s ^ 1]), ((i - 1) >> 1) & 1, TC_WAIT))) {
         fence_after_sync();
         readout(s ^ 1);
-      } else if (lane == 0) {
-        abort_flag = 1;
+      } else {
+        ok = false;
+        if (lane == 0) abort_flag = 1;
       }
     }
-    if (ok && c + 1 < nc) stage(c + 1);
-    publish();
+    if (ok && i + 2 < nc) fetch(c + 2);  // into the stage of step c - 1 and the raw buffer of step c
+    if (ok && i + 1 < nc) {
+      if (i + 2 < nc) asm volatile("cp.async.wait_group 1;" ::: "memory");
+      else asm volatile("cp.async.wait_group 0;" ::: "memory");
+      split(c + 1);
+    }
+    barrier();
     ok = abort_flag == 0;
   }
   if (ok && nc > 0) {
-    const int c = nc - 1;
-    if (__all_sync(0xffffffffu, mbar_wait(smem_u32(&mbar[c & 1]), (c >> 1) & 1, TC_WAIT))) {
+    const int i = nc - 1;
+    if (__all_sync(0xffffffffu, mbar_spin(smem_u32(&mbar[i & 1]), (i >> 1) & 1, TC_WAIT))) {
       fence_after_sync();
-      readout(c & 1);
+      readout(i & 1);
     } else if (lane == 0) {
       abort_flag = 1;
     }
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
   ok = abort_flag == 0;
   if (!ok) {
     if (tid == 0) atomicExch(status, 1);
-  } else {
+  } else if (nc > 0) {
     const int r = m0 + 32 * w + lane;
     if (r < M) {
       const double al = alpha ? alpha[r] : 1.0;
       TC* crow = C + coff[r] + n0;
+      if (gridDim.z > 1) {
+        // a part of a split K: added in FP64 into the scratch row r (k_tc_finish moves it into C)
+        double* srow = scratch + (int64_t)r * N + n0;
 #pragma unroll
-      for (int j = 0; j < TC_BN; j++)
-        if (n0 + j < N) store_out(crow + j, al * (double)run[j], acc);
+        for (int j = 0; j < TC_BN; j++)
+          if (n0 + j < N) atomicAdd(srow + j, al * (double)run[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < TC_BN; j++)
+          if (n0 + j < N) store_out(crow + j, al * (double)run[j], acc);
+      }
     }
   }
   if (w == 0) tmem_dealloc(tm, 128);
+}
+
+// C[coff[r] + j] (=|+=) scratch[r][j] for the rows of a split-K tensor-core GEMM, scratch cleared for its
+// next use
+template <class TC>
+__global__ void k_tc_finish(int M, int N, double* __restrict__ scratch, TC* __restrict__ C,
+                            const int64_t* __restrict__ coff, int acc) {
+  const int64_t total = (int64_t)M * N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / N), j = (int)(e % N);
+    store_out(C + coff[r] + j, scratch[e], acc);
+    scratch[e] = 0.0;
+  }
 }
 
 // out[j][k] = E[k][j] for the real form E ([KR][NR]) of B, TF32 head and tail, zero outside E, for
@@ -621,15 +688,40 @@ void tgemm_tc(const TGemm& g, const float* A, const float* Bth, const float* Btl
   if (g.M <= 0 || g.N <= 0) return;
   XREQUIRE(g.status && g.astep % 2 == 0 && ldbt % TC_BK == 0, XFMM_ERR_UNSUPPORTED,
            "tensor-core translation: status flag and aligned rows required");
-  const dim3 grid((g.M + TC_BM - 1) / TC_BM, (g.N + TC_BN - 1) / TC_BN);
+  // K split over blockIdx.z for levels with few row tiles (two CTAs per SM, about two waves), in parts
+  // of at least 8 steps; only where C is accumulated into (the parts are added with atomics)
+  const int mt = (g.M + TC_BM - 1) / TC_BM, nt = (g.N + TC_BN - 1) / TC_BN, nsteps = (g.K + TC_BK - 1) / TC_BK;
+  int kz = 1;
+  if (g.accumulate) {
+    const int want = (XFMM_TC_KSPLIT_CTAS + mt * nt - 1) / (mt * nt);
+    kz = std::max(1, std::min(std::min(want, nsteps / 8), XFMM_TC_KSPLIT_MAX));
+  }
+  if (kz > 1) {
+    // the parts meet in an FP64 scratch ([M][N], zero between uses), then one pass adds it into C
+    XREQUIRE(g.scratch && g.scratch_len >= (int64_t)g.M * g.N, XFMM_ERR_UNSUPPORTED,
+             "split tensor-core translation: scratch too small");
+  }
+  const dim3 grid(mt, nt, kz);
   auto go = [&](auto kern) {
     XCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
     kern<<<grid, TC_NT, TC_SMEM, s>>>(g.M, g.N, g.K, A, g.aoff, Bth, Btl, ldbt, g.alpha, C, g.coff, g.accumulate,
-                                      g.status);
+                                      g.status, g.scratch);
   };
   if (g.astep % 4 == 0) go(k_tgemm_tc<TC, 16>);
   else go(k_tgemm_tc<TC, 8>);
   XLAUNCH();
+  if (kz > 1) {
+    k_tc_finish<TC><<<tg_blocks((int64_t)g.M * g.N), 256, 0, s>>>(g.M, g.N, g.scratch, C, g.coff, g.accumulate);
+    XLAUNCH();
+  }
+}
+// the FP64 scratch (doubles) a split tgemm_tc of M x N needs, 0 when it does not split
+int64_t tgemm_tc_scratch(int M, int N, int K, int accumulate) {
+  const int mt = (M + TC_BM - 1) / TC_BM, nt = (N + TC_BN - 1) / TC_BN, nsteps = (K + TC_BK - 1) / TC_BK;
+  if (!accumulate || M <= 0 || N <= 0) return 0;
+  const int want = (XFMM_TC_KSPLIT_CTAS + mt * nt - 1) / (mt * nt);
+  const int kz = std::max(1, std::min(std::min(want, nsteps / 8), XFMM_TC_KSPLIT_MAX));
+  return kz > 1 ? (int64_t)M * N : 0;
 }
 template void tgemm_tc<float>(const TGemm&, const float*, const float*, const float*, int64_t, float*, cudaStream_t);
 template void tgemm_tc<double>(const TGemm&, const float*, const float*, const float*, int64_t, double*, cudaStream_t);

@@ -230,6 +230,8 @@ struct TGemm {
   int accumulate = 0;
   int64_t astep = 0;  // every A offset is a multiple of astep elements (alignment of the A rows)
   int* status = nullptr;  // device flag set by a tensor-core GEMM whose bounded wait ran out
+  double* scratch = nullptr;  // FP64 [M][N] for a split tensor-core GEMM, zero between uses
+  int64_t scratch_len = 0;
 };
 template <class TA, class TC>
 void tgemm_f64(const TGemm& g, const TA* A, const double* B, TC* C, cudaStream_t s);
@@ -238,6 +240,7 @@ void tgemm_tf32(const TGemm& g, const float* A, const float* Bh, const float* Bl
 template <class TC>
 void tgemm_tc(const TGemm& g, const float* A, const float* Bth, const float* Btl, int64_t ldbt, TC* C,
               cudaStream_t s);
+int64_t tgemm_tc_scratch(int M, int N, int K, int accumulate);
 void expand_operator_t(const void* B, bool b_single, int K, int N, int64_t ldb, bool cplx, int npad, int64_t ldbt,
                        float* ohi, float* olo, cudaStream_t s);
 void expand_operator(const void* B, bool b_single, int K, int N, int64_t ldb, bool cplx, double* o64, float* ohi,
