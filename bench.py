@@ -349,8 +349,9 @@ def cpu_baseline(n, steps=3, warmup=1):
 
 def run_batched(args):
     """256 independent Laplace systems (N log-uniform in [2e3, 2e5], half cube, half Plummer), p=6,
-    ncrit=64, mixed precision: one CUDA-graph replay of all evaluates vs the same evaluates launched
-    one system at a time.  Aggregate particles/s over all systems."""
+    ncrit=64, mixed precision: one CUDA-graph replay of the batched evaluate (per-system stages on
+    concurrent streams, one persistent near-field kernel over every system's target leaves) vs the
+    same evaluates launched one system at a time.  Aggregate particles/s over all systems."""
     import torch
     import exafmm.laplace as L
     from exafmm.batch import BatchedFmm, batched_workload
@@ -359,7 +360,7 @@ def run_batched(args):
     t0 = time.perf_counter()
     b = BatchedFmm(systems, lambda: L.LaplaceFmm(6, 64, precision="mixed"))
     setup_s = time.perf_counter() - t0
-    b.autotune()  # concurrent streams inside the graph, then the sparse Hadamard's tiles per CTA
+    b.autotune()  # streams x persistent near-field shape, then the sparse Hadamard's tiles per CTA
 
     def timed(fn):
         for _ in range(args.warmup):
@@ -385,7 +386,10 @@ def run_batched(args):
                        "n_total": ntot, "l2_flush": "none (total working set ~3 GB > L2)"},
             "per_problem_launches": {"value": ntot / (ms_each * 1e-3) / 1e6, "ms_per_step": ms_each},
             "graph_speedup": ms_each / ms_graph, "setup_s": setup_s,
-            "graph_streams": b.nstreams, "autotune_ms_per_replay": {str(k): round(v, 3) for k, v in b.tuning.items()},
+            "graph_streams": b.nstreams, "near_ctas_per_sm": b.near_ctas_per_sm,
+            "near_targets_per_lane": b.near_tpl,
+            "autotune_ms_per_replay": {"streams=%d,ctas_per_sm=%d,tpl=%d" % k: round(v, 3)
+                                       for k, v in b.tuning.items()},
             "sparse_hadamard_tiles_per_cta": b.tiles_per_cta,
             "autotune_tiles_ms_per_replay": {str(k): round(v, 3) for k, v in b.tile_tuning.items()},
             "clocks": clk.summary()}

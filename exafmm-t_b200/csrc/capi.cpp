@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "xfmm_internal.h"
 
@@ -318,6 +319,46 @@ xfmm_status xfmm_set_tuning(xfmm_tree* tree, int option, int value) {
     XREQUIRE(option == XFMM_TUNE_SPARSE_HADAMARD_TILES_PER_CTA, XFMM_ERR_ARG, "unknown tuning option");
     XREQUIRE(value >= 0 && value <= 64, XFMM_ERR_ARG, "sparse Hadamard tiles per CTA must be 0..64");
     tree->t.hadr_tpc = value;
+  });
+}
+
+xfmm_status xfmm_batch_create(xfmm_fmm* const* fmms, xfmm_tree* const* trees, int n, void* stream, xfmm_batch** out) {
+  return guarded([&] {
+    XREQUIRE(fmms && trees && out && n > 0, XFMM_ERR_ARG, "null argument");
+    std::vector<xfmm::Fmm*> f(n);
+    std::vector<xfmm::Tree*> t(n);
+    for (int k = 0; k < n; k++) {
+      XREQUIRE(fmms[k] && trees[k], XFMM_ERR_ARG, "null system handle");
+      f[k] = &fmms[k]->f;
+      t[k] = &trees[k]->t;
+    }
+    *out = reinterpret_cast<xfmm_batch*>(xfmm::batch_create(f.data(), t.data(), n, S(stream)));
+  });
+}
+
+xfmm_status xfmm_batch_evaluate(xfmm_batch* b, const double* const* charges, double* const* outs, int nstreams,
+                                void* stream) {
+  return guarded([&] {
+    XREQUIRE(b && outs, XFMM_ERR_ARG, "null argument");
+    xfmm::batch_evaluate(reinterpret_cast<xfmm::Batch*>(b), charges, outs, nstreams, S(stream));
+  });
+}
+
+xfmm_status xfmm_batch_set_tuning(xfmm_batch* b, int option, int value) {
+  return guarded([&] {
+    XREQUIRE(b, XFMM_ERR_ARG, "null argument");
+    xfmm::batch_set_tuning(reinterpret_cast<xfmm::Batch*>(b), option, value);
+  });
+}
+
+xfmm_status xfmm_batch_free(xfmm_batch* b) {
+  return guarded([&] { xfmm::batch_free(reinterpret_cast<xfmm::Batch*>(b)); });
+}
+
+xfmm_status xfmm_batch_schedule(const int64_t* sizes, int n, int nstreams, int* stream_of) {
+  return guarded([&] {
+    XREQUIRE((sizes && stream_of) || n == 0, XFMM_ERR_ARG, "null argument");
+    xfmm::batch_schedule(sizes, n, nstreams, stream_of);
   });
 }
 

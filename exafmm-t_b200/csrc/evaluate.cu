@@ -802,10 +802,11 @@ __global__ void __launch_bounds__(128) k_close_scan(NearArgs a, unsigned long lo
 // For each close pair: the exact FP64 contribution (r == 0 skipped, laplace.h:57) in place of the bounded
 // FP32 one that k_near_lap_f2 added (recomputed with the same operations; the gradient's FP32 product is
 // taken exactly in FP64, as the fused multiply-add took it).
-__global__ void k_close_fix(const int4* __restrict__ pairs, int64_t n, NearArgs a) {
+__global__ void k_close_fix(const int4* __restrict__ pairs, int64_t n, NearArgs a1, const NearArgs* __restrict__ args) {
   const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
   const int4 pr = pairs[k];
+  const NearArgs& a = args ? args[pr.w] : a1;  // one system, or system pr.w of a batch
   const double4 tv = a.trg4[pr.x], sv = a.src4[pr.y], cn = a.center[pr.z];
   const float dc2 = near_close2(cn.w);
   const float3 tr = leaf_rel(tv, cn), sr = leaf_rel(sv, cn);
@@ -2607,6 +2608,8 @@ void find_close_pairs(Workspace& ws, const NearArgs& na, int n_eval, cudaStream_
   ws.n_close = (int64_t)n;
 }
 
+constexpr int DOWN_PRE = 1, DOWN_NEAR = 2, DOWN_FAR = 4, DOWN_ALL = 7;
+
 // ------------------------------------------------------------------ engine, per kernel and precision
 template <int KER, class R>
 struct Engine {
@@ -2863,7 +2866,55 @@ struct Engine {
     }
   }
 
-  static void downward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s) {
+  static NearArgs near_args(Fmm& f, Tree& t, Workspace& ws) {
+    return NearArgs{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.n_eval_leafs, t.sbeg.p, t.tbeg.p,
+                    t.p2p_off.p,    t.p2p.p,   t.center.p,  t.src4.p,  t.trg4.p,       t.src_qim.p, ws.out.p,
+                    f.k_re,         f.k_im};
+  }
+
+  // phases: DOWN_PRE (P2L, M2L, L2L, L2P check-to-equivalent), DOWN_NEAR (P2P), DOWN_FAR (M2P + L2P
+  // evaluation, added to the near field's values); an evaluate runs all three in this order
+  static void downward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int phases = DOWN_ALL) {
+    const int n = f.nsurf;
+    if (phases & DOWN_PRE) downward_pre(f, t, ws, s);
+    if (t.n_eval_leafs && (phases & DOWN_NEAR)) {
+      NearArgs na = near_args(f, t, ws);
+      if constexpr (KER == K_LAPLACE && sizeof(R) == 4) {
+        if (ws.n_close < 0) find_close_pairs(ws, na, t.n_eval_leafs, s);
+        k_near_lap_f2<<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
+        XLAUNCH();
+        ws.launches++;
+        if (ws.n_close > 0) {
+          k_close_fix<<<nblk(ws.n_close, 256), 256, 0, s>>>(ws.close_pairs.p, ws.n_close, na, nullptr);
+          XLAUNCH();
+          ws.launches++;
+        }
+      } else {
+        k_near<KER, R><<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
+        XLAUNCH();
+        ws.launches++;
+      }
+    }
+    if (phases & DOWN_NEAR) XCUDA(cudaEventRecord(ws.ev[8], s));
+    if (t.n_eval_leafs && (phases & DOWN_FAR)) {
+      EvalArgs a{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.level.p,     t.n_eval_leafs, t.sbeg.p,
+                 t.tbeg.p,       t.center.p, t.src4.p,   t.trg4.p,  t.src_qim.p,   t.p2p_off.p,    t.m2p_off.p,
+                 t.p2p.p,        t.m2p.p,   f.surf_base.p, n,        ws.up.p,       ws.eq.p,        ws.out.p,
+                 f.k_re,         f.k_im,    1,           1,         0,             1};
+      const int blocks = nblk(t.n_eval_leafs, EVAL_WARPS);
+      a.do_near = 0;
+      a.accumulate = 1;
+      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
+        k_far_lap<W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
+      else
+        k_eval<KER, double, W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
+      XLAUNCH();
+      ws.launches++;
+    }
+    if (phases & DOWN_FAR) XCUDA(cudaEventRecord(ws.ev[7], s));
+  }
+
+  static void downward_pre(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s) {
     const int n = f.nsurf;
     // P2L (X list) into downward check potentials
     if (t.n_p2l_nodes) {
@@ -2923,45 +2974,6 @@ struct Engine {
       }
     }
     XCUDA(cudaEventRecord(ws.ev[6], s));
-    // Target evaluation: the near field (P2P) in the working precision (FP32 with hi/lo coordinates when
-    // mixed), then the far field (M2P + L2P: sums of cancelling equivalent charges) in FP64, accumulated.
-    if (t.n_eval_leafs) {
-      EvalArgs a{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.level.p,     t.n_eval_leafs, t.sbeg.p,
-                 t.tbeg.p,       t.center.p, t.src4.p,   t.trg4.p,  t.src_qim.p,   t.p2p_off.p,    t.m2p_off.p,
-                 t.p2p.p,        t.m2p.p,   f.surf_base.p, n,        ws.up.p,       ws.eq.p,        ws.out.p,
-                 f.k_re,         f.k_im,    1,           1,         0,             1};
-      const int blocks = nblk(t.n_eval_leafs, EVAL_WARPS);
-      NearArgs na{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.n_eval_leafs, t.sbeg.p, t.tbeg.p,
-                  t.p2p_off.p,    t.p2p.p,   t.center.p,  t.src4.p,  t.trg4.p,       t.src_qim.p, ws.out.p,
-                  f.k_re,         f.k_im};
-      if constexpr (KER == K_LAPLACE && sizeof(R) == 4) {
-        if (ws.n_close < 0) find_close_pairs(ws, na, t.n_eval_leafs, s);
-        k_near_lap_f2<<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
-        XLAUNCH();
-        ws.launches++;
-        if (ws.n_close > 0) {
-          k_close_fix<<<nblk(ws.n_close, 256), 256, 0, s>>>(ws.close_pairs.p, ws.n_close, na);
-          XLAUNCH();
-          ws.launches++;
-        }
-      } else {
-        k_near<KER, R><<<nblk(t.n_eval_leafs, 4), 128, 0, s>>>(na);
-        XLAUNCH();
-        ws.launches++;
-      }
-      XCUDA(cudaEventRecord(ws.ev[8], s));
-      a.do_near = 0;
-      a.accumulate = 1;
-      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
-        k_far_lap<W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
-      else
-        k_eval<KER, double, W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
-      XLAUNCH();
-      ws.launches++;
-    } else {
-      XCUDA(cudaEventRecord(ws.ev[8], s));
-    }
-    XCUDA(cudaEventRecord(ws.ev[7], s));
   }
 };
 
@@ -3035,6 +3047,254 @@ void downward_pass(Fmm& f, Tree& t, cudaStream_t s) {
   check_ready(f, t);
   Workspace& ws = workspace(f, t, s);
   dispatch(f, [&](auto e) { decltype(e)::downward(f, t, ws, s); });
+}
+
+// ================================================================ many systems in one evaluate
+// Persistent near field over the target leaves of every system of a batch: each warp takes work items
+// (system, target leaf) from one queue (a global counter, zeroed before the launch) in the order of
+// `items` (largest pair count first) until it runs dry.  tpl: the largest number of targets a lane holds
+// (1 or 2), the height of the warp's target tile.
+__global__ void __launch_bounds__(128, XFMM_NEARF2_MINB)
+    k_near_lap_f2_queue(const NearArgs* __restrict__ args, const int2* __restrict__ items, int64_t nitems,
+                        unsigned int* __restrict__ counter, int tpl) {
+  __shared__ NearSmemF2 sm[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (;;) {
+    unsigned int k = 0;
+    if (lane == 0) k = atomicAdd(counter, 1u);
+    k = __shfl_sync(0xffffffffu, k, 0);
+    if ((int64_t)k >= nitems) break;
+    const int2 it = items[k];
+    const NearArgs& a = args[it.x];
+    const int node = a.leafs[a.eval_leafs[it.y]];
+    const int T = a.ntrgs[node];
+    if (T <= 32 || tpl == 1) near_leaf_lap_f2<1>(a, node, lane, sm[wid]);
+    else near_leaf_lap_f2<2>(a, node, lane, sm[wid]);
+    __syncwarp();
+  }
+}
+template <int KER, class R>
+__global__ void __launch_bounds__(128, XFMM_NEAR_MINB)
+    k_near_queue(const NearArgs* __restrict__ args, const int2* __restrict__ items, int64_t nitems,
+                 unsigned int* __restrict__ counter, int tpl) {
+  __shared__ NearSmem<R> sm[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (;;) {
+    unsigned int k = 0;
+    if (lane == 0) k = atomicAdd(counter, 1u);
+    k = __shfl_sync(0xffffffffu, k, 0);
+    if ((int64_t)k >= nitems) break;
+    const int2 it = items[k];
+    const NearArgs& a = args[it.x];
+    const int node = a.leafs[a.eval_leafs[it.y]];
+    const int T = a.ntrgs[node];
+    if (sizeof(R) == 4 && T > 32 && tpl >= 2) near_leaf<KER, R, 2>(a, node, lane, sm[wid]);
+    else near_leaf<KER, R, 1>(a, node, lane, sm[wid]);
+    __syncwarp();
+  }
+}
+// pairs of one system, tagged with its index in .w, appended to a batch list
+__global__ void k_tag_pairs(const int4* __restrict__ src, int64_t n, int sys, int4* __restrict__ dst) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < n) {
+    int4 v = src[k];
+    v.w = sys;
+    dst[k] = v;
+  }
+}
+
+struct Batch {
+  std::vector<Fmm*> fmm;
+  std::vector<Tree*> tree;
+  int kernel = 0, precision = 0;
+  DBuf<NearArgs> args;
+  DBuf<int2> items;
+  int64_t nitems = 0;
+  DBuf<unsigned int> counter;
+  DBuf<int4> close;
+  int64_t nclose = 0;
+  std::vector<int> order;  // systems, most bodies first (dealt to the streams in this order)
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;
+  int near_ctas_per_sm = 0, near_tpl = 2;  // tuning (0: the kernel's resident limit)
+  ~Batch() {
+    for (auto e : events) cudaEventDestroy(e);
+    for (auto st : streams) cudaStreamDestroy(st);
+  }
+};
+
+Batch* batch_create(Fmm** fmms, Tree** trees, int n, cudaStream_t s) {
+  XREQUIRE(n > 0, XFMM_ERR_ARG, "a batch needs at least one system");
+  auto* b = new Batch();
+  try {
+    b->kernel = fmms[0]->kernel;
+    b->precision = fmms[0]->precision;
+    std::vector<NearArgs> hargs(n);
+    std::vector<std::pair<int64_t, int2>> work;
+    std::vector<int64_t> bodies(n);
+    for (int k = 0; k < n; k++) {
+      Fmm& f = *fmms[k];
+      Tree& t = *trees[k];
+      XREQUIRE(f.kernel == b->kernel && f.precision == b->precision, XFMM_ERR_ARG,
+               "the systems of a batch share one kernel and one precision");
+      check_ready(f, t);
+      Workspace& ws = workspace(f, t, s);
+      b->fmm.push_back(&f);
+      b->tree.push_back(&t);
+      dispatch(f, [&](auto e) { hargs[k] = decltype(e)::near_args(f, t, ws); });
+      bodies[k] = t.ntrg;
+      // work items: target leaves, costed by their pair counts
+      std::vector<int64_t> poff = t.p2p_off.download(s);
+      std::vector<int> pl = t.p2p.download(s, (size_t)t.np2p);
+      std::vector<int> el = t.eval_leafs.download(s, (size_t)t.n_eval_leafs);
+      for (int i = 0; i < t.n_eval_leafs; i++) {
+        const int node = t.h_leafs[el[i]];
+        int64_t ns = 0;
+        for (int64_t e = poff[node]; e < poff[node + 1]; e++) ns += t.h_nsrcs[pl[e]];
+        work.push_back({(int64_t)t.h_ntrgs[node] * ns, make_int2(k, i)});
+      }
+      if (f.kernel == XFMM_LAPLACE && f.mixed() && ws.n_close < 0 && t.n_eval_leafs > 0)
+        find_close_pairs(ws, hargs[k], t.n_eval_leafs, s);
+      if (f.kernel == XFMM_LAPLACE && f.mixed()) b->nclose += std::max<int64_t>(ws.n_close, 0);
+    }
+    std::stable_sort(work.begin(), work.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<int2> items(work.size());
+    for (size_t i = 0; i < work.size(); i++) items[i] = work[i].second;
+    b->nitems = (int64_t)items.size();
+    b->items.upload(items, s);
+    b->args.upload(hargs, s);
+    b->counter.alloc(1);
+    if (b->nclose > 0) {
+      b->close.alloc((size_t)b->nclose);
+      int64_t off = 0;
+      for (int k = 0; k < n; k++) {
+        Workspace& ws = *trees[k]->ws[fmms[k]->precision];
+        if (ws.n_close <= 0) continue;
+        k_tag_pairs<<<nblk(ws.n_close, 256), 256, 0, s>>>(ws.close_pairs.p, ws.n_close, k, b->close.p + off);
+        XLAUNCH();
+        off += ws.n_close;
+      }
+    }
+    b->order.resize(n);
+    for (int k = 0; k < n; k++) b->order[k] = k;
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return bodies[x] > bodies[y]; });
+    XCUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    delete b;
+    throw;
+  }
+  return b;
+}
+
+void batch_free(Batch* b) { delete b; }
+
+void batch_schedule(const int64_t* sizes, int n, int nstreams, int* stream_of) {
+  XREQUIRE(n >= 0 && nstreams >= 1, XFMM_ERR_ARG, "batch schedule needs n >= 0 and nstreams >= 1");
+  std::vector<int> order(n);
+  for (int k = 0; k < n; k++) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return sizes[x] > sizes[y]; });
+  std::vector<int64_t> load(std::max(1, std::min(nstreams, std::max(n, 1))), 0);
+  for (int k : order) {
+    const int j = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    stream_of[k] = j;
+    load[j] += sizes[k];
+  }
+}
+
+void batch_set_tuning(Batch* b, int option, int value) {
+  if (option == XFMM_BATCH_NEAR_CTAS_PER_SM) {
+    XREQUIRE(value >= 0 && value <= 32, XFMM_ERR_ARG, "CTAs per SM out of range (0..32)");
+    b->near_ctas_per_sm = value;
+  } else if (option == XFMM_BATCH_NEAR_TARGETS_PER_LANE) {
+    XREQUIRE(value == 1 || value == 2, XFMM_ERR_ARG, "targets per lane must be 1 or 2");
+    b->near_tpl = value;
+  } else {
+    XREQUIRE(false, XFMM_ERR_ARG, "unknown batch tuning option");
+  }
+}
+
+// One evaluate of every system: charges (device, caller's order; null: keep the current ones) in,
+// potentials and gradients out (device, caller's order).  The per-system stages before and after the
+// near field run on `nstreams` streams forked from s (systems dealt largest first, each to the stream
+// with the fewest bodies so far); the near field of all systems is one persistent launch on s.
+void batch_evaluate(Batch* b, const double* const* charges, double* const* outs, int nstreams, cudaStream_t s) {
+  const int n = (int)b->fmm.size();
+  nstreams = std::max(1, std::min(nstreams, n));
+  while ((int)b->streams.size() < nstreams) {
+    cudaStream_t st;
+    XCUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    b->streams.push_back(st);
+  }
+  while (b->events.size() < (size_t)2 * (nstreams + 1)) {
+    cudaEvent_t e;
+    XCUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->events.push_back(e);
+  }
+  std::vector<int64_t> sizes(n);
+  for (int k = 0; k < n; k++) sizes[k] = b->tree[k]->ntrg;
+  std::vector<int> stream_of(n);
+  batch_schedule(sizes.data(), n, nstreams, stream_of.data());
+  std::vector<std::vector<int>> lists(nstreams);
+  for (int k : b->order) lists[stream_of[k]].push_back(k);
+  auto fork_join = [&](int evbase, auto&& body) {
+    if (nstreams == 1) {
+      for (int k : lists[0]) body(k, s);
+      return;
+    }
+    XCUDA(cudaEventRecord(b->events[evbase], s));
+    for (int j = 0; j < nstreams; j++) {
+      XCUDA(cudaStreamWaitEvent(b->streams[j], b->events[evbase], 0));
+      for (int k : lists[j]) body(k, b->streams[j]);
+      XCUDA(cudaEventRecord(b->events[evbase + 1 + j], b->streams[j]));
+      XCUDA(cudaStreamWaitEvent(s, b->events[evbase + 1 + j], 0));
+    }
+  };
+  fork_join(0, [&](int k, cudaStream_t st) {
+    Fmm& f = *b->fmm[k];
+    Tree& t = *b->tree[k];
+    if (charges && charges[k]) set_charges(f, t, charges[k], true, st);
+    clear_values(f, t, st);
+    Workspace& ws = workspace(f, t, st);
+    dispatch(f, [&](auto e) {
+      decltype(e)::upward(f, t, ws, st);
+      decltype(e)::downward(f, t, ws, st, DOWN_PRE);
+    });
+  });
+  // the near field of every system: one persistent launch draining the work queue
+  if (b->nitems > 0) {
+    int dev = 0, nsm = 148;
+    XCUDA(cudaGetDevice(&dev));
+    XCUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    XCUDA(cudaMemsetAsync(b->counter.p, 0, sizeof(unsigned int), s));
+    const bool lapf2 = b->kernel == XFMM_LAPLACE && b->precision == XFMM_MIXED;
+    auto launch = [&](auto kern) {
+      int per_sm = 0;
+      XCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0));
+      if (b->near_ctas_per_sm > 0) per_sm = std::min(per_sm, b->near_ctas_per_sm);
+      const int64_t need = (b->nitems + 3) / 4;
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * nsm, need));
+      kern<<<grid, 128, 0, s>>>(b->args.p, b->items.p, b->nitems, b->counter.p, b->near_tpl);
+      XLAUNCH();
+    };
+    if (lapf2) launch(k_near_lap_f2_queue);
+    else if (b->kernel == XFMM_LAPLACE) launch(k_near_queue<K_LAPLACE, double>);
+    else if (b->kernel == XFMM_MODIFIED_HELMHOLTZ)
+      b->precision == XFMM_MIXED ? launch(k_near_queue<K_YUKAWA, float>) : launch(k_near_queue<K_YUKAWA, double>);
+    else
+      b->precision == XFMM_MIXED ? launch(k_near_queue<K_HELMHOLTZ, float>) : launch(k_near_queue<K_HELMHOLTZ, double>);
+    if (lapf2 && b->nclose > 0) {
+      NearArgs none{};
+      k_close_fix<<<nblk(b->nclose, 256), 256, 0, s>>>(b->close.p, b->nclose, none, b->args.p);
+      XLAUNCH();
+    }
+  }
+  fork_join(nstreams + 1, [&](int k, cudaStream_t st) {
+    Fmm& f = *b->fmm[k];
+    Tree& t = *b->tree[k];
+    Workspace& ws = workspace(f, t, st);
+    dispatch(f, [&](auto e) { decltype(e)::downward(f, t, ws, st, DOWN_FAR); });
+    get_values(f, t, outs[k], st);
+  });
 }
 
 // Device times of the last upward + downward pass (ms): 0 P2M, 1 M2M, 2 P2L, 3 M2L, 4 L2L,

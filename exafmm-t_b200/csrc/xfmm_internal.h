@@ -246,6 +246,13 @@ void expand_operator_t(const void* B, bool b_single, int K, int N, int64_t ldb, 
 void expand_operator(const void* B, bool b_single, int K, int N, int64_t ldb, bool cplx, double* o64, float* ohi,
                      float* olo, cudaStream_t s);
 void prepare_translation_operands(const Fmm& f, LevelOps& op, cudaStream_t s);
+// evaluate.cu: many systems in one evaluate (xfmm_batch_*)
+struct Batch;
+Batch* batch_create(Fmm** fmms, Tree** trees, int n, cudaStream_t s);
+void batch_free(Batch* b);
+void batch_schedule(const int64_t* sizes, int n, int nstreams, int* stream_of);
+void batch_set_tuning(Batch* b, int option, int value);
+void batch_evaluate(Batch* b, const double* const* charges, double* const* outs, int nstreams, cudaStream_t s);
 // capi.cpp: record the message returned by xfmm_last_error() on this thread
 void set_last_error(const char* msg);
 

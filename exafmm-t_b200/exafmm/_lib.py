@@ -41,6 +41,11 @@ SIGNATURES = [
     ("xfmm_tree_dump", i32, [vp] * 17),
     ("xfmm_stage_times", i32, [vp, vp, vp]),
     ("xfmm_set_tuning", i32, [vp, i32, i32]),
+    ("xfmm_batch_create", i32, [vp, vp, i32, vp, ctypes.POINTER(vp)]),
+    ("xfmm_batch_evaluate", i32, [vp, vp, vp, i32, vp]),
+    ("xfmm_batch_set_tuning", i32, [vp, i32, i32]),
+    ("xfmm_batch_free", i32, [vp]),
+    ("xfmm_batch_schedule", i32, [vp, i32, i32, vp]),
     ("xfmm_gradient_p2p", i32, [i32, f64, f64, i32, vp, i64, vp, vp, i64, vp, i32, vp]),
     ("xfmm_verify", i32, [vp, vp, i32, vp, vp]),
     ("xfmm_gradient_p2p_noalloc", i32, [i32, f64, f64, i32, vp, i64, vp, vp, i64, vp, vp]),

@@ -2,21 +2,21 @@
 reference, which evaluates one system per call).
 
 Each system gets its own Fmm object (operators depend on the system's bounding box), tree, lists and
-device buffers for its charges and results.  One evaluate of every system (charges in, potentials
-and gradients out, all device-resident) is captured once into a CUDA graph and then replayed with a
-single launch; ``evaluate_each`` runs the same calls one system after another without the graph.
-Charges are read from ``charges[i]`` (device tensors) at every replay, so new values are picked up
-by writing into those tensors in place.  The work runs on the batch's own stream, ordered after the
-caller's current stream, which in turn waits for it: results may be read on the current stream.
+device buffers for its charges and results.  The systems are held by one native batch (xfmm_batch_*):
+one evaluate of every system runs each system's stages before and after its near field on concurrent
+streams forked from the batch stream (largest systems first, each to the least-loaded stream), and the
+near field of all systems as one persistent kernel that drains a work queue of (system, target leaf)
+items, largest first, followed by one launch of the close-pair corrections of all systems.  That
+evaluate is captured once into a CUDA graph and replayed with a single launch; ``evaluate_each`` runs
+the per-system evaluates one after another without the graph or the batch.  Charges are read from
+``charges[i]`` (device tensors) at every replay, so new values are picked up by writing into those
+tensors in place.  The work runs on the batch's own stream, ordered after the caller's current stream,
+which in turn waits for it: results may be read on the current stream.
 
-Inside the graph the systems may run concurrently: ``capture(nstreams)`` forks the batch stream into
-``nstreams`` streams (each system's calls stay in order on one of them; systems are dealt, largest
-first, to the stream with the fewest bodies so far) and joins them again, so the small grids of small
-systems share the GPU instead of running one after another.  Every system owns its operators, tree,
-work buffers and library handles (cuBLAS with a fixed workspace), so nothing is shared between the
-streams.  ``autotune()`` captures the graph for each candidate stream count, times replays on the
-device and keeps the fastest; then, at that stream count, it does the same for each candidate tile
-shape of the sparse M2L Hadamard (target tiles per CTA, set on every tree through xfmm_set_tuning).
+``autotune()`` captures the graph for each candidate stream count and each candidate tile shape of the
+persistent near-field kernel (CTAs per SM; targets per lane, the height of a warp's target tile), times
+replays on the device and keeps the fastest; then, with those, it does the same for the sparse M2L
+Hadamard's target tiles per CTA (set on every tree through xfmm_set_tuning).
 """
 import ctypes
 
@@ -24,6 +24,8 @@ import numpy as np
 import torch
 
 from . import _core, _lib
+
+NEAR_CTAS_PER_SM, NEAR_TARGETS_PER_LANE = 1, 2  # include/xfmm.h XFMM_BATCH_NEAR_*
 
 
 class BatchedFmm:
@@ -46,64 +48,70 @@ class BatchedFmm:
             self.outs.append(torch.zeros((len(coords), width), dtype=torch.float64, device="cuda"))
         self.n = [len(c) for c, _ in systems]
         self.stream = torch.cuda.Stream()
-        self._side = []
+        k = len(self.n)
+        fa = (ctypes.c_void_p * k)(*[f._h.value for f in self.fmms])
+        ta = (ctypes.c_void_p * k)(*[t._h.value for t in self.trees])
+        self._qp = (ctypes.c_void_p * k)(*[q.data_ptr() for q in self.charges])
+        self._op = (ctypes.c_void_p * k)(*[o.data_ptr() for o in self.outs])
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().xfmm_batch_create(fa, ta, k, ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(h)))
+        self._b = h
         self.graph = None
         self.nstreams = 1
-        self.tuning = {}        # stream count -> ms per replay
+        self.near_ctas_per_sm, self.near_tpl = 0, 2  # persistent near field (0: as many CTAs as fit)
+        self.tuning = {}        # (streams, CTAs per SM, targets per lane) -> ms per replay
         self.tiles_per_cta = 0  # sparse Hadamard tiles per CTA on every tree (0: the library default)
-        self.tile_tuning = {}   # tiles per CTA -> ms per replay, at the chosen stream count
+        self.tile_tuning = {}   # tiles per CTA -> ms per replay, with the chosen shape
 
-    def _enqueue(self, stream_handle, order=None):
+    def __del__(self):
+        b = getattr(self, "_b", None)
+        if b is not None and b.value:
+            self.graph = None
+            _lib.lib().xfmm_batch_free(b)
+            self._b = None
+
+    def set_near_shape(self, ctas_per_sm, targets_per_lane):
+        """Tile shape of the persistent near-field kernel; recapture after."""
+        L = _lib.lib()
+        _lib.check(L.xfmm_batch_set_tuning(self._b, NEAR_CTAS_PER_SM, int(ctas_per_sm)))
+        _lib.check(L.xfmm_batch_set_tuning(self._b, NEAR_TARGETS_PER_LANE, int(targets_per_lane)))
+        self.near_ctas_per_sm, self.near_tpl = int(ctas_per_sm), int(targets_per_lane)
+
+    def _batch(self, nstreams):
+        _lib.check(_lib.lib().xfmm_batch_evaluate(self._b, self._qp, self._op, int(nstreams),
+                                                  ctypes.c_void_p(self.stream.cuda_stream)))
+
+    def _enqueue(self, stream_handle):
         L = _lib.lib()
         st = ctypes.c_void_p(stream_handle)
-        for i in (range(len(self.n)) if order is None else order):
+        for i in range(len(self.n)):
             fmm, tree, q, out = self.fmms[i], self.trees[i], self.charges[i], self.outs[i]
             _lib.check(L.xfmm_set_charges(fmm._h, tree._h, ctypes.c_void_p(q.data_ptr()), 1, st))
             _lib.check(L.xfmm_evaluate(fmm._h, tree._h, ctypes.c_void_p(out.data_ptr()), 1, st))
 
-    def _deal(self, nstreams):
-        """Systems per stream: largest first, each to the stream with the fewest bodies so far."""
-        load, lists = [0] * nstreams, [[] for _ in range(nstreams)]
-        for i in sorted(range(len(self.n)), key=lambda i: -self.n[i]):
-            k = min(range(nstreams), key=lambda k: load[k])
-            lists[k].append(i)
-            load[k] += self.n[i]
-        return [l for l in lists if l]
-
-    def _enqueue_forked(self, nstreams):
-        """All systems on nstreams streams forked from and joined back into the batch stream."""
-        if nstreams <= 1:
-            self._enqueue(self.stream.cuda_stream)
-            return
-        while len(self._side) < nstreams:
-            self._side.append(torch.cuda.Stream())
-        fork = torch.cuda.Event()
-        fork.record(self.stream)
-        for k, order in enumerate(self._deal(nstreams)):
-            side = self._side[k]
-            side.wait_event(fork)
-            self._enqueue(side.cuda_stream, order)
-            join = torch.cuda.Event()
-            join.record(side)
-            self.stream.wait_event(join)
-
     def evaluate_each(self):
-        """One evaluate per system, launched one after another on the batch stream (no graph)."""
+        """One evaluate per system, launched one after another on the batch stream (no graph, no batch)."""
         self.stream.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(self.stream):
             self._enqueue(self.stream.cuda_stream)
         torch.cuda.current_stream().wait_stream(self.stream)
         return self.outs
 
+    def evaluate_batch(self, nstreams=None):
+        """One batched evaluate of every system (no graph)."""
+        self.stream.wait_stream(torch.cuda.current_stream())
+        self._batch(self.nstreams if nstreams is None else nstreams)
+        torch.cuda.current_stream().wait_stream(self.stream)
+        return self.outs
+
     def capture(self, nstreams=1):
-        """Capture one evaluate of every system into a CUDA graph, the systems spread over nstreams
-        concurrent streams.  The first evaluate of each system (which sizes its work buffers) runs
-        here, before the capture begins."""
-        self.evaluate_each()
+        """Capture one batched evaluate of every system into a CUDA graph, the per-system stages spread
+        over nstreams concurrent streams.  One evaluate runs here first, outside the capture."""
+        self.evaluate_batch(nstreams)
         self.stream.synchronize()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=self.stream):
-            self._enqueue_forked(int(nstreams))
+            self._batch(int(nstreams))
         self.graph = g
         self.nstreams = int(nstreams)
         return g
@@ -125,12 +133,31 @@ class BatchedFmm:
             tree.set_tuning("sparse_hadamard_tiles_per_cta", value)
         self.tiles_per_cta = int(value)
 
-    def autotune(self, candidates=(1, 2, 4, 8, 16, 32), reps=3, tile_candidates=(1, 2, 4, 8)):
-        """Capture the graph for each stream count in candidates, time `reps` replays of each on the
-        device (after one untimed replay) and keep the fastest graph; then, at that stream count, the
-        same for each sparse-Hadamard tiles-per-CTA value in tile_candidates.  self.tuning maps each
-        stream count, self.tile_tuning each tile value, to its milliseconds per replay."""
-        self._autotune_streams(candidates, reps)
+    def autotune(self, candidates=(4, 8, 16, 32), near_shapes=((0, 2), (4, 2), (0, 1), (2, 2)), reps=3,
+                 tile_candidates=(1, 2, 4, 8)):
+        """Capture the graph for each stream count in candidates and each persistent near-field shape
+        (CTAs per SM, targets per lane) in near_shapes, time `reps` replays of each on the device (after
+        one untimed replay) and keep the fastest; then, with those, the same for each sparse-Hadamard
+        tiles-per-CTA value in tile_candidates.  self.tuning maps each (streams, CTAs per SM, targets per
+        lane), self.tile_tuning each tile value, to its milliseconds per replay."""
+        best = None
+        for ns in candidates:
+            ns = max(1, min(int(ns), len(self.n)))
+            for cps, tpl in near_shapes:
+                key = (ns, int(cps), int(tpl))
+                if key in self.tuning:
+                    continue
+                self.set_near_shape(cps, tpl)
+                g = self.capture(ns)
+                self.tuning[key] = self._time_graph(g, reps)
+                if best is None or self.tuning[key] < self.tuning[best]:
+                    best = key
+                del g
+                self.graph = None
+        if best is None:
+            best = min(self.tuning, key=self.tuning.get)
+        self.set_near_shape(best[1], best[2])
+        self.capture(best[0])
         if tile_candidates:
             best_ms, best_tiles = None, self.tiles_per_cta
             for tiles in tile_candidates:
@@ -141,24 +168,6 @@ class BatchedFmm:
                     best_ms, best_tiles = self.tile_tuning[int(tiles)], int(tiles)
             self.set_tiles_per_cta(best_tiles)
             self.capture(self.nstreams)
-        return self.nstreams
-
-    def _autotune_streams(self, candidates, reps):
-        best = None
-        for ns in candidates:
-            ns = max(1, min(int(ns), len(self.n)))
-            if ns in self.tuning:
-                continue
-            g = self.capture(ns)
-            self.tuning[ns] = self._time_graph(g, reps)
-            if best is None or self.tuning[ns] < self.tuning[best[0]]:
-                best = (ns, g)
-            else:
-                del g
-        if best is not None:
-            self.nstreams, self.graph = best
-        else:  # every candidate timed before: recapture the fastest
-            self.capture(min(self.tuning, key=self.tuning.get))
         return self.nstreams
 
     def replay(self):

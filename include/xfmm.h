@@ -138,6 +138,33 @@ enum {
  * an unknown option or a value out of range. */
 xfmm_status xfmm_set_tuning(xfmm_tree* tree, int option, int value);
 
+/* Many independent systems evaluated together (no counterpart in the reference, which evaluates one
+ * system per call).  A batch holds systems that share one kernel and one precision, each set up as for
+ * xfmm_evaluate (tree, lists, M2L setup, precompute); the handles must outlive the batch and keep their
+ * trees.  xfmm_batch_evaluate runs one evaluate of every system: charges[k] (device, caller's source
+ * order; NULL array or entry: keep the system's current charges) in, outs[k] (device, caller's target
+ * order) out.  Each system's stages before and after its near field run on `nstreams` concurrent streams
+ * forked from `stream` (largest systems first, each to the least-loaded stream); the near field of all
+ * systems is one persistent kernel draining a work queue of (system, target leaf) items, largest first,
+ * and the exact close-pair corrections of all systems one more launch.  Asynchronous on `stream`, no
+ * allocation: it may be captured into a CUDA graph (after one evaluate outside the capture). */
+typedef struct xfmm_batch xfmm_batch;
+enum {
+  /* persistent near field: CTAs per SM (0: as many as fit; 1..32) */
+  XFMM_BATCH_NEAR_CTAS_PER_SM = 1,
+  /* persistent near field: most targets a lane holds, the height of a warp's target tile (1 or 2) */
+  XFMM_BATCH_NEAR_TARGETS_PER_LANE = 2
+};
+xfmm_status xfmm_batch_create(xfmm_fmm* const* fmms, xfmm_tree* const* trees, int n, void* stream, xfmm_batch** out);
+xfmm_status xfmm_batch_evaluate(xfmm_batch* batch, const double* const* charges, double* const* outs, int nstreams,
+                                void* stream);
+xfmm_status xfmm_batch_set_tuning(xfmm_batch* batch, int option, int value);
+xfmm_status xfmm_batch_free(xfmm_batch* batch);
+/* The stream each system of a batch of n runs its per-system stages on, as xfmm_batch_evaluate deals
+ * them: systems by size (sizes[k], descending, ties in index order), each to the stream with the least
+ * total size so far (ties: the lowest stream); min(nstreams, n) streams.  Host only, no device work. */
+xfmm_status xfmm_batch_schedule(const int64_t* sizes, int n, int nstreams, int* stream_of);
+
 /* Direct near-field kernel over raw arrays: out += potential and gradient at trg from (src, q); out is
  * ntrg x 4 doubles (Laplace, modified Helmholtz) or ntrg x 8 (Helmholtz: 4 interleaved complex values).
  * precision selects the FP64 or FP32 device kernel. */
