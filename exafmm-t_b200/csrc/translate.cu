@@ -316,7 +316,9 @@ __global__ void __launch_bounds__(TG_NT, 4) k_tgemm_tf32(int M, int N, int K, co
 // Per step: the rows' A pieces arrive raw by cp.async two steps ahead (16 bytes per lane, coalesced), are
 // split into TF32 head and tail one step ahead and stored into shared memory as K-major core matrices
 // (8 rows x 16 bytes, 128 contiguous bytes each); the operator's head and tail (pre-split, transposed to
-// [N][K], zero-padded to whole tiles) arrive by cp.async in the same layout, two steps ahead.  One
+// [N][K], zero-padded to whole tiles) arrive by cp.async in the same layout, two steps ahead.  The proxy
+// fence that hands a split step to the tensor core is issued before the next step's copies, so that it
+// has none of this thread's copies in flight to wait for (measured: 5% faster M2M and L2L).  One
 // elected lane of warp 0 issues the step's six MMAs (M128 N64 K8; Ah Bt + At Bh + Ah Bh per half step,
 // the first into a fresh accumulator) into one of two TMEM accumulators and commits them to that
 // accumulator's mbarrier.  While they run, every warp reads the previous step's accumulator back (its 32
@@ -519,13 +521,17 @@ __global__ void __launch_bounds__(TC_NT, 2)
         if (lane == 0) abort_flag = 1;
       }
     }
-    if (ok && i + 2 < nc) fetch(c + 2);  // into the stage of step c - 1 and the raw buffer of step c
+    // step c + 1 is split and made visible to the tensor core (proxy fence) before step c + 2's copies are
+    // issued, so that the fence has no copies of this thread in flight to wait for
     if (ok && i + 1 < nc) {
-      if (i + 2 < nc) asm volatile("cp.async.wait_group 1;" ::: "memory");
-      else asm volatile("cp.async.wait_group 0;" ::: "memory");
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
       split(c + 1);
     }
-    barrier();
+    fence_proxy_async_smem();
+    if (ok && i + 2 < nc) fetch(c + 2);  // into the stage of step c - 1 and the raw buffer of step c
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
     ok = abort_flag == 0;
   }
   if (ok && nc > 0) {
