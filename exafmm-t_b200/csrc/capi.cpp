@@ -168,9 +168,10 @@ xfmm_status xfmm_precompute(xfmm_fmm* fmm, xfmm_tree* tree, void* stream) {
     XREQUIRE(tree->t.r0 > 0, XFMM_ERR_STATE, "precompute before build_tree");
     f.r0 = tree->t.r0;
     f.depth = tree->t.depth;
-    // cached operators are reused when r0 (and depth, for the per-level kernels) match
-    // (the load_matrix check of fmm_scale_invariant.h:113-148, keyed on everything here)
-    const bool same = f.precomputed && f.pre_r0 == f.r0 &&
+    // cached operators are reused when r0 (and depth, for the per-level kernels) match (the load_matrix
+    // check of fmm_scale_invariant.h:113-148, keyed on everything here); the scale-invariant Laplace
+    // operators serve any r0 (the evaluate applies the ratio of the radii, op_scale in evaluate.cu)
+    const bool same = f.precomputed && (f.kernel == XFMM_LAPLACE ? f.pre_r0 > 0 : f.pre_r0 == f.r0) &&
                       (f.kernel == XFMM_LAPLACE || f.pre_depth >= tree->t.depth);
     if (!same) xfmm::precompute(f, tree->t.depth, S(stream));
   });

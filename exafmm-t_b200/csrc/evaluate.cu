@@ -861,6 +861,15 @@ __global__ void __launch_bounds__(128, XFMM_NEAR_MINB) k_near(NearArgs a) {
 
 // ================================================================ P2M check potentials and P2L
 // Potential at `n` surface points (base * b around centre cn) from body range(s); warp per node.
+// The Laplace operators are scale-invariant: computed for root radius pre_r0, they serve a tree of root
+// radius r0 = lambda pre_r0 unchanged except for a factor lambda on the check potentials that come straight
+// from bodies (P2M, P2L).  With the kernel 1 / (4 pi r), K(lambda x, lambda y) = K(x, y) / lambda: the
+// check-to-equivalent pseudo-inverse scales by lambda, M2M and L2L (pseudo-inverse times kernel matrix)
+// not at all, and the M2L kernel table by 1 / lambda.  Scaling the P2M check potentials by lambda gives the
+// true upward densities; the M2L then yields lambda times the true downward check potentials, which P2L
+// must match, and the unscaled pseudo-inverse of L2P maps them to the true downward densities.
+inline double op_scale(const Fmm& f, const Tree& t) { return f.kernel == XFMM_LAPLACE ? t.r0 / f.pre_r0 : 1.0; }
+
 struct SurfPotArgs {
   const int* nodes;  // node per warp (P2M: leafs; P2L: p2l_nodes)
   int count;
@@ -874,6 +883,7 @@ struct SurfPotArgs {
   void* out;           // working values
   int out_by_node;     // 0: row = warp index (P2M chk[pos]); 1: row = node (P2L into dn, accumulate)
   double k_re, k_im;
+  double scale;        // 1 / (4 pi) x op_scale(f, t): the Green's function constant and the operators' r0 scale
 };
 
 template <int KER, class R>
@@ -915,7 +925,7 @@ __global__ void __launch_bounds__(128) k_surf_pot(SurfPotArgs a) {
           const V4 sx = s_xyz[wid][j];
           g.pot(px - sx.x, py - sx.y, pz - sx.z, s_q[wid][j], acc);
         }
-        acc = vscale(acc, (typename Base<Q>::type)INV4PI);
+        acc = vscale(acc, (typename Base<Q>::type)a.scale);
         out[k] = first ? acc : vadd(out[k], acc);
       }
       first = false;
@@ -995,7 +1005,7 @@ __global__ void __launch_bounds__(128) k_surf_pot_lap_f2(SurfPotArgs a) {
       for (int i = 0; i < SP_KB; i++) {
         const int k = k0 + lane + 32 * i;
         if (k < n) {
-          const float o = (acc[i].x + acc[i].y) * (float)INV4PI;
+          const float o = (acc[i].x + acc[i].y) * (float)a.scale;
           out[k] = first ? o : out[k] + o;
         }
       }
@@ -2625,7 +2635,8 @@ struct Engine {
     // P2M: check potentials of every leaf, then the pinv (UC2E) GEMM per leaf level
     if (t.nleafs) {
       SurfPotArgs a{t.leafs.p,  t.nleafs, t.nsrcs.p,     nullptr,  t.level.p, t.sbeg.p,   nullptr, t.center.p,
-                    t.src4.p,   t.src_qim.p, f.surf_base.p, n,      2.95,      ws.chk.p, 0,         f.k_re, f.k_im};
+                    t.src4.p,   t.src_qim.p, f.surf_base.p, n,      2.95,      ws.chk.p, 0,         f.k_re, f.k_im,
+                    INV4PI * op_scale(f, t)};
       if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
         k_surf_pot_lap_f2<<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
       else
@@ -2920,7 +2931,7 @@ struct Engine {
     if (t.n_p2l_nodes) {
       SurfPotArgs a{t.p2l_nodes.p, t.n_p2l_nodes, t.nsrcs.p,     t.p2l.p, t.level.p, t.sbeg.p, t.p2l_off.p, t.center.p,
                     t.src4.p,      t.src_qim.p,   f.surf_base.p, n,       1.05,      ws.dn.p,  1,           f.k_re,
-                    f.k_im};
+                    f.k_im,        INV4PI * op_scale(f, t)};
       k_surf_pot<KER, R><<<nblk(t.n_p2l_nodes, 4), 128, 0, s>>>(a);
       XLAUNCH();
       ws.launches++;
@@ -2995,7 +3006,8 @@ void check_ready(const Fmm& f, const Tree& t) {
   XREQUIRE(t.lists_built, XFMM_ERR_STATE, "evaluate before build_list");
   XREQUIRE(t.m2l_ready, XFMM_ERR_STATE, "evaluate before M2L_setup");
   XREQUIRE(f.precomputed, XFMM_ERR_STATE, "evaluate before precompute");
-  XREQUIRE(f.pre_r0 == t.r0, XFMM_ERR_STATE, "operators were precomputed for another root radius");
+  XREQUIRE(f.pre_r0 == t.r0 || f.kernel == XFMM_LAPLACE, XFMM_ERR_STATE,
+           "operators were precomputed for another root radius");
   XREQUIRE(f.kernel == XFMM_LAPLACE || f.pre_depth >= t.depth, XFMM_ERR_STATE,
            "operators were precomputed for a shallower tree");
   XREQUIRE(t.nsurf_lists == f.nsurf, XFMM_ERR_STATE, "lists were built for another expansion order");

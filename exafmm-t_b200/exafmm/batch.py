@@ -1,8 +1,10 @@
 """Many independent particle systems evaluated as one captured CUDA graph (no counterpart in the
 reference, which evaluates one system per call).
 
-Each system gets its own Fmm object (operators depend on the system's bounding box), tree, lists and
-device buffers for its charges and results.  The systems are held by one native batch (xfmm_batch_*):
+Each system gets its own tree, lists and device buffers for its charges and results.  Laplace systems
+share one Fmm object: its scale-invariant operators, precomputed once for the first system's root radius,
+serve every other radius (the evaluate scales the body-to-check potentials by the ratio of the radii);
+the other kernels' operators depend on the radius, so each of those systems gets its own Fmm object.  The systems are held by one native batch (xfmm_batch_*):
 one evaluate of every system runs each system's stages before and after its near field on concurrent
 streams forked from the batch stream (largest systems first, each to the least-loaded stream), and the
 near field of all systems as one persistent kernel that drains a work queue of (system, target leaf)
@@ -31,10 +33,14 @@ NEAR_CTAS_PER_SM, NEAR_TARGETS_PER_LANE = 1, 2  # include/xfmm.h XFMM_BATCH_NEAR
 class BatchedFmm:
     """systems: list of (coords (n, 3) array, charges (n,) array); fmm_factory() -> a new Fmm object."""
 
-    def __init__(self, systems, fmm_factory, nonadaptive_depth=None):
+    def __init__(self, systems, fmm_factory, nonadaptive_depth=None, share_operators=True):
         self.fmms, self.trees, self.charges, self.outs = [], [], [], []
+        shared = None
         for coords, q in systems:
-            fmm = fmm_factory()
+            # the scale-invariant Laplace operators serve every system of the batch (one precompute)
+            fmm = shared if shared is not None else fmm_factory()
+            if share_operators and fmm.kernel == "laplace":
+                shared = fmm
             dtype = np.complex128 if fmm.kernel == "helmholtz" else np.float64
             src = _core.init_sources(coords, np.asarray(q, dtype), fmm.kernel)
             tree = _core.setup(src, _core.init_targets(coords), fmm, nonadaptive_depth)
@@ -62,6 +68,11 @@ class BatchedFmm:
         self.tuning = {}        # (streams, CTAs per SM, targets per lane) -> ms per replay
         self.tiles_per_cta = 0  # sparse Hadamard tiles per CTA on every tree (0: the library default)
         self.tile_tuning = {}   # tiles per CTA -> ms per replay, with the chosen shape
+
+    @property
+    def n_operator_sets(self):
+        """Distinct Fmm objects (operator sets) the systems use."""
+        return len({id(f) for f in self.fmms})
 
     def __del__(self):
         b = getattr(self, "_b", None)

@@ -104,3 +104,19 @@ def test_batched_systems_match_direct_sums():
         pe, ge = orc.rel_l2(o.cpu().numpy()[s], orc.direct("laplace", x, q, x[s]))
         assert pe < 1e-4 and ge < 1e-3, (pe, ge)
 
+
+
+def test_laplace_systems_share_one_operator_set():
+    systems, b = _batch("fp64")
+    assert b.n_operator_sets == 1 and len({round(t.dump()["r0"], 12) for t in b.trees}) > 1
+    # each system against its own freshly precomputed operators (the reference's per-radius precompute)
+    import exafmm.laplace as lap
+    seq = [o.clone() for o in b.evaluate_each()]
+    torch.cuda.synchronize()
+    for (x, q), o in list(zip(systems, seq))[:3]:
+        fmm = lap.LaplaceFmm(6, 64, precision="fp64")
+        tree = lap.setup(lap.init_sources(x, q), lap.init_targets(x), fmm)
+        own = lap.evaluate(tree, fmm)
+        ref = o.cpu().numpy()
+        rel = np.linalg.norm(own - ref) / np.linalg.norm(own)
+        assert rel < 1e-9, rel
