@@ -1059,93 +1059,102 @@ void transpose(const CT* in, CT* out, int64_t R, int64_t C, cudaStream_t s) {
 
 // Hadamard product per frequency (fmm_scale_invariant.h:343-399; intrinsics.h matmult_8x8x2):
 //   out[f][t][tc] = sum_ipos sum_sc T[ipos][f][sc*8 + tc] * in[f][src(t, ipos)][sc]
-// FP64 form: a CTA owns a tile of HAD_TT targets and HAD_KC frequencies.  Each warp owns 32 of the
-// tile's targets at one frequency and streams their (target, source, relative position) pairs in
-// rounds of 32 lanes; rounds are built on the host so that no target occurs twice in a round, hence
-// the shared-memory accumulators need no atomics and no block barrier between positions (the sums
-// are taken in a fixed order), and each lane prefetches its next round while computing the current
-// one.  The mixed path's forms run on the tensor cores (k_hadamard_dt, k_hadamard_rt below).
-constexpr int HAD_TT = 128;  // targets per CTA (4 warps x 32)
-constexpr int HAD_ST = 9;    // accumulator row stride (values): conflict-free for consecutive targets
+// The FP64 path's form runs on the FP64 tensor cores (k_hadamard_d64), the mixed path's forms on the
+// TF32 tensor cores (k_hadamard_dt, k_hadamard_rt below).
 
-template <class CT> struct HadKC;
-template <> struct HadKC<double2> { static constexpr int KC = 1; };
+// Hadamard product of the FP64 path on the FP64 tensor cores (DMMA, mma.sync m8n8k4 f64), dense form for
+// every target: per frequency, D[target][16] = A[target][26 x 16] B[26 x 16][16] as in k_hadamard_dt,
+// accumulated in FP64 by the tensor core across the positions.  A warp owns HAD64_TW tiles of 8 targets;
+// per (tile, position) eight DMMAs (4 reduction steps x 2 output halves) add the position's products to the
+// tile's accumulators.  The reduction index of step c is input real 4 t + c, so that a lane (g, t) supplies
+// the reals 4 t .. 4 t + 3 of its target g's source spectrum (32 contiguous bytes) and receives the output
+// component 4 h + t (re, im) of target g.  A position none of a tile's 8 targets occupies is skipped (warp
+// ballot); sources are loaded one position ahead.
+constexpr int HAD64_NT = 256, HAD64_TW = 2;
+constexpr int HAD64_TT = (HAD64_NT / 32) * 8 * HAD64_TW;  // targets per CTA
+constexpr size_t HAD64_SMEM = (size_t)26 * 4 * 2 * 32 * sizeof(double);
 
-__device__ __forceinline__ void had_mac8(const double2* __restrict__ M, const double2* v, double2* o) {
-#pragma unroll
-  for (int sc = 0; sc < 8; sc++)
-#pragma unroll
-    for (int tc = 0; tc < 8; tc++) vfma(o[tc], M[sc * 8 + tc], v[sc]);
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
 }
 
-template <class CT> struct HadM { using type = CT; };
-
-template <class CT>
-__device__ __forceinline__ void had_load8(const CT* __restrict__ p, CT* v) {
-#pragma unroll
-  for (int i = 0; i < 8; i++) v[i] = p[i];
-}
-
-template <class CT>
-__global__ void __launch_bounds__(128 * HadKC<CT>::KC) k_hadamard(const CT* __restrict__ T, const CT* __restrict__ in,
-                                                                   CT* __restrict__ out,
-                                                                   const int* __restrict__ grp_off,
-                                                                   const int2* __restrict__ ent, int nsrc, int ntrg,
-                                                                   int nfreq) {
-  constexpr int KC = HadKC<CT>::KC;
-  using MT = typename HadM<CT>::type;
+// tab: [26][ld] compact source index of target k at each position (-1: empty or padding); rows: [ld]
+// output row of target k (-1: padding); ld a multiple of HAD64_TT
+__global__ void __launch_bounds__(HAD64_NT, 2)
+    k_hadamard_d64(const double2* __restrict__ T, const double2* __restrict__ in, double2* __restrict__ out,
+                   const int* __restrict__ tab, int ld, const int* __restrict__ rows, int nsrc, int ntrg, int nfreq) {
+  // sB[((ipos * 4 + c) * 2 + h) * 32 + lane] = B[input real 4 t + c][output real 8 h + g] for that lane
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  MT* sM = reinterpret_cast<MT*>(smem_raw);                  // [KC][26][64]
-  CT* sAcc = reinterpret_cast<CT*>(sM + KC * 26 * 64);        // [KC][HAD_TT][HAD_ST]
-  const int tile = blockIdx.x, f0 = blockIdx.y * KC, tid = threadIdx.x;
-  const int lane = tid & 31, wid = tid >> 5;
-  const int kk = wid >> 2, grp = wid & 3;
-  const int t0 = tile * HAD_TT, nt = min(HAD_TT, ntrg - t0);
-  for (int e = tid; e < KC * 26 * 64; e += blockDim.x) {
-    const int j = e & 63, ipos = (e >> 6) % 26, k = e / (26 * 64);
-    const int f = min(f0 + k, nfreq - 1);
-    const CT m = T[((int64_t)ipos * nfreq + f) * 64 + j];
-    sM[e] = m;
+  double* sB = reinterpret_cast<double*>(smem_raw);
+  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int e = tid; e < 26 * 4 * 2 * 32; e += HAD64_NT) {
+    const int ln = e & 31, h = (e >> 5) & 1, c = (e >> 6) & 3, ipos = e >> 8;
+    const int gg = ln >> 2, tt = ln & 3;
+    const int sc = 2 * tt + (c >> 1), ri = c & 1;      // input real 4 tt + c: component sc, re / im
+    const int o = 8 * h + gg, tc = o >> 1, ro = o & 1;  // output real o: component tc, re / im
+    const double2 m = T[((int64_t)ipos * nfreq + f) * 64 + sc * 8 + tc];
+    // output re <- (Re m, -Im m) . (in re, in im); output im <- (Im m, Re m)
+    sB[e] = ro == 0 ? (ri == 0 ? m.x : -m.y) : (ri == 0 ? m.y : m.x);
   }
-  for (int e = tid; e < KC * HAD_TT * HAD_ST; e += blockDim.x) sAcc[e] = vzero<CT>();
   __syncthreads();
-  const int f = f0 + kk;
-  if (f < nfreq) {
-    const CT* inf = in + (int64_t)f * nsrc * 8;
-    const MT* Mk = sM + kk * 26 * 64;
-    CT* acc = sAcc + kk * HAD_TT * HAD_ST;
-    const int e0 = grp_off[tile * 4 + grp], e1 = grp_off[tile * 4 + grp + 1];
-    int2 cur = e0 + lane < e1 ? ent[e0 + lane] : make_int2(-1, 0);
-    CT v[8];
-    if (cur.x >= 0) had_load8<CT>(inf + (int64_t)cur.x * 8, v);
-    for (int e = e0; e < e1; e += 32) {
-      // prefetch the next round
-      int2 nxt = e + 32 + lane < e1 ? ent[e + 32 + lane] : make_int2(-1, 0);
-      CT w[8];
-      if (nxt.x >= 0) had_load8<CT>(inf + (int64_t)nxt.x * 8, w);
-      if (cur.x >= 0) {
-        const int ipos = cur.y >> 8, lt = cur.y & 255;
-        CT o[8];
+  const int g = lane >> 2, t = lane & 3;
+  const double2* inf = in + (int64_t)f * nsrc * 8 + 2 * t;  // components 2 t, 2 t + 1: reals 4 t .. 4 t + 3
+  auto load4 = [&](int sidx) {
+    if (sidx < 0) return make_double4(0.0, 0.0, 0.0, 0.0);
+    const double2 u = __ldg(inf + (int64_t)sidx * 8), v = __ldg(inf + (int64_t)sidx * 8 + 1);
+    return make_double4(u.x, u.y, v.x, v.y);
+  };
+  const int base = blockIdx.x * HAD64_TT + wid * 8 * HAD64_TW + g;  // this lane's target in tile j: base + 8 j
+  double acc[HAD64_TW][2][2];
+  int src[HAD64_TW], srcn[HAD64_TW];
+  double4 x[HAD64_TW];
 #pragma unroll
-        for (int i = 0; i < 8; i++) o[i] = vzero<CT>();
-        had_mac8(Mk + ipos * 64, v, o);
-        CT* q = acc + lt * HAD_ST;
+  for (int j = 0; j < HAD64_TW; j++) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) q[i] = vadd(q[i], o[i]);
-      }
-      __syncwarp();
-      cur = nxt;
+    for (int h = 0; h < 2; h++) acc[j][h][0] = acc[j][h][1] = 0.0;
+    src[j] = tab[base + 8 * j];
+    srcn[j] = tab[ld + base + 8 * j];
+    x[j] = load4(src[j]);
+  }
+  for (int ipos = 0; ipos < 26; ipos++) {
+    // next position's source pieces, and the position after's source indices
+    double4 xn[HAD64_TW];
+    int srcnn[HAD64_TW];
 #pragma unroll
-      for (int i = 0; i < 8; i++) v[i] = w[i];
+    for (int j = 0; j < HAD64_TW; j++) {
+      xn[j] = ipos + 1 < 26 ? load4(srcn[j]) : make_double4(0.0, 0.0, 0.0, 0.0);
+      srcnn[j] = ipos + 2 < 26 ? tab[(ipos + 2) * ld + base + 8 * j] : -1;
+    }
+    double b[4][2];
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) b[c][h] = sB[((ipos * 4 + c) * 2 + h) * 32 + lane];
+#pragma unroll
+    for (int j = 0; j < HAD64_TW; j++) {
+      if (__ballot_sync(0xffffffffu, src[j] >= 0) == 0u) continue;  // no target of the tile here
+      const double a[4] = {x[j].x, x[j].y, x[j].z, x[j].w};
+#pragma unroll
+      for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) dmma_884(acc[j][h], a[c], b[c][h]);
+    }
+#pragma unroll
+    for (int j = 0; j < HAD64_TW; j++) {
+      src[j] = srcn[j];
+      srcn[j] = srcnn[j];
+      x[j] = xn[j];
     }
   }
-  __syncthreads();
-  for (int k = 0; k < KC; k++) {
-    const int ff = f0 + k;
-    if (ff >= nfreq) break;
-    CT* of = out + ((int64_t)ff * ntrg + t0) * 8;
-    const CT* acc = sAcc + k * HAD_TT * HAD_ST;
-    for (int e = tid; e < nt * 8; e += blockDim.x) of[e] = acc[(e >> 3) * HAD_ST + (e & 7)];
+  double2* of = out + (int64_t)f * ntrg * 8;
+#pragma unroll
+  for (int j = 0; j < HAD64_TW; j++) {
+    const int row = rows[base + 8 * j];
+    if (row < 0) continue;
+#pragma unroll
+    for (int h = 0; h < 2; h++) of[(int64_t)row * 8 + 4 * h + t] = make_double2(acc[j][h][0], acc[j][h][1]);
   }
 }
 
@@ -2285,8 +2294,6 @@ struct Workspace {
   DBuf<char> grid, specA, specB;
   std::vector<cufftHandle> fwd, bwd;
   // Hadamard tiling: per group, tiles of TT targets; CSR over (tile, ipos) of (local target, source)
-  DBuf<int> had_off;
-  DBuf<int2> had_pairs;
   std::vector<int> had_tile0;  // first tile of each group (ngroups + 1)
   // FP32: sparse targets in the round form (per tile the range of rounds and HADR_TT output rows; per
   // round its relative position and HADR_RW pairs), dense targets in the dense form (per group a
@@ -2296,8 +2303,7 @@ struct Workspace {
   DBuf<int> hadd_tab, hadd_row;
   std::vector<int64_t> hadd_tab0, hadd_row0;
   std::vector<int> hadd_ld;
-  size_t hadamard_smem = 0;
-  bool hadt_attr = false, hadrt_attr = false, hadc_attr = false;
+  bool hadt_attr = false, hadrt_attr = false, hadc_attr = false, had64_attr = false;
   // dense Hadamard targets on tcgen05 (k_hadamard_dc) instead of mma.sync (k_hadamard_dt): chosen when the
   // workspace is created, by XFMM_HADAMARD_TCGEN05=1 in the environment
   bool had_tc5 = false;
@@ -2541,47 +2547,37 @@ Workspace& workspace(Fmm& f, Tree& t, cudaStream_t s) {
     W.hadd_tab.upload(dtab, s);
     W.hadd_row.upload(drow, s);
   } else {
-    // per group of M2L targets: tiles of HAD_TT targets, 4 warp groups of 32 targets; each warp group's
-    // pairs (ordered by relative position) packed into rounds of 32 lanes with no repeated target,
-    // padded with src = -1.  Entry: {source index, (ipos << 8) | target index within the tile}.
-    std::vector<int> off;
-    std::vector<int2> ent;
+    // FP64: every target in the dense form on the FP64 tensor cores (k_hadamard_d64): per group a [26][ld]
+    // source table and ld output rows, targets level by level (Morton order inside a level), padded to
+    // whole CTA tiles
+    std::vector<int> dtab, drow;
     W.had_tile0.assign(ng + 1, 0);
-    int ntiles = 0;
+    W.hadd_tab0.assign(ng, 0);
+    W.hadd_row0.assign(ng, 0);
+    W.hadd_ld.assign(ng, 0);
     for (int g = 0; g < ng; g++) {
-      W.had_tile0[g] = ntiles;
       const int tb = t.m2l_trg_off[g], te = t.m2l_trg_off[g + 1];
-      for (int t0 = tb; t0 < te; t0 += HAD_TT, ntiles++) {
-        for (int wg = 0; wg < 4; wg++) {
-          off.push_back((int)ent.size());
-          const int a0 = t0 + 32 * wg, a1 = std::min(te, a0 + 32);
-          std::vector<int2> round;
-          uint64_t used = 0;
-          auto flush = [&]() {
-            if (round.empty()) return;
-            for (auto& r : round) ent.push_back(r);
-            for (size_t k = round.size(); k < 32; k++) ent.push_back(make_int2(-1, 0));
-            round.clear();
-            used = 0;
-          };
-          for (int ipos = 0; ipos < 26; ipos++)
-            for (int tt = a0; tt < a1; tt++) {
-              const int sidx = t.h_m2l_tab[26 * (size_t)tt + ipos];
-              if (sidx < 0) continue;
-              const int lw = tt - a0;
-              if ((used >> lw) & 1 || round.size() == 32) flush();
-              round.push_back(make_int2(sidx, (ipos << 8) | (tt - t0)));
-              used |= (uint64_t)1 << lw;
-            }
-          flush();
-        }
+      std::vector<int> all;
+      for (int tt = tb; tt < te; tt++) all.push_back(tt);
+      std::stable_sort(all.begin(), all.end(),
+                       [&](int a, int b) { return t.h_level[t.h_m2l_trg[a]] < t.h_level[t.h_m2l_trg[b]]; });
+      const int ld = (int)((all.size() + HAD64_TT - 1) / HAD64_TT) * HAD64_TT;
+      W.hadd_ld[g] = ld;
+      W.hadd_tab0[g] = (int64_t)dtab.size();
+      W.hadd_row0[g] = (int64_t)drow.size();
+      dtab.resize(dtab.size() + (size_t)26 * ld, -1);
+      drow.resize(drow.size() + ld, -1);
+      for (size_t k = 0; k < all.size(); k++) {
+        const int tt = all[k];
+        drow[W.hadd_row0[g] + k] = tt - tb;
+        for (int ipos = 0; ipos < 26; ipos++)
+          dtab[W.hadd_tab0[g] + (size_t)ipos * ld + k] = t.h_m2l_tab[26 * (size_t)tt + ipos];
       }
     }
-    W.had_tile0[ng] = ntiles;
-    off.push_back((int)ent.size());
-    if (ent.empty()) ent.push_back(make_int2(-1, 0));
-    W.had_off.upload(off, s);
-    W.had_pairs.upload(ent, s);
+    if (dtab.empty()) dtab.push_back(-1);
+    if (drow.empty()) drow.push_back(-1);
+    W.hadd_tab.upload(dtab, s);
+    W.hadd_row.upload(drow, s);
   }
   for (auto& e : W.ev) XCUDA(cudaEventCreate(&e));
   W.m2l_ev.resize(4 * (size_t)ng);
@@ -2786,18 +2782,18 @@ struct Engine {
           ws.launches++;
         }
       } else {
-        constexpr int KC = HadKC<CT>::KC;
-        using MT = typename HadM<CT>::type;
-        const size_t smem = (size_t)KC * 26 * 64 * sizeof(MT) + (size_t)KC * HAD_TT * HAD_ST * sizeof(CT);
-        if (ws.hadamard_smem < smem) {
-          XCUDA(cudaFuncSetAttribute(k_hadamard<CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-          ws.hadamard_smem = smem;
+        XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
+        if (ws.hadd_ld[g] > 0) {
+          if (!ws.had64_attr) {
+            XCUDA(cudaFuncSetAttribute(k_hadamard_d64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HAD64_SMEM));
+            ws.had64_attr = true;
+          }
+          k_hadamard_d64<<<dim3(ws.hadd_ld[g] / HAD64_TT, nfreq), HAD64_NT, HAD64_SMEM, s>>>(
+              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+              ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
+          XLAUNCH();
+          ws.launches++;
         }
-        k_hadamard<CT><<<dim3(ntiles, (nfreq + KC - 1) / KC), 128 * KC, smem, s>>>(
-            T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.had_off.p + (int64_t)ws.had_tile0[g] * 4,
-            ws.had_pairs.p, ns, nt, nfreq);
-        XLAUNCH();
-        ws.launches++;
       }
       XCUDA(cudaEventRecord(ev[2], s));
       // inverse DFT of specA [f][t][c] to the downward check potentials (fmm_scale_invariant.h:606-646)
