@@ -485,10 +485,11 @@ __device__ __forceinline__ void near_leaf(const NearArgs& a, int node, int lane,
           const R hx = (R)dx, hy = (R)dy, hz = (R)dz;
           const R qi = CPLX ? (R)a.src_qim[si] : (R)0;
           sm.hi[lane] = {hx, hy, hz, (R)sv.w};
-          sm.lo[lane] = {(R)(dx - (double)hx), (R)(dy - (double)hy), (R)(dz - (double)hz), qi};
+          if constexpr (HILO || CPLX)
+            sm.lo[lane] = {(R)(dx - (double)hx), (R)(dy - (double)hy), (R)(dz - (double)hz), qi};
         } else {
           sm.hi[lane] = {(R)1e3, (R)1e3, (R)1e3, (R)0};  // zero-charge padding, far from every target
-          sm.lo[lane] = {(R)0, (R)0, (R)0, (R)0};
+          if constexpr (HILO || CPLX) sm.lo[lane] = {(R)0, (R)0, (R)0, (R)0};
         }
         __syncwarp();
         Q p[TPL], gx[TPL], gy[TPL], gz[TPL];
@@ -498,7 +499,8 @@ __device__ __forceinline__ void near_leaf(const NearArgs& a, int node, int lane,
         for (int jj = 0; jj < nper; jj++) {
           const int j = jj * G2 + sub;
           const auto h = sm.hi[j];
-          const auto l = sm.lo[j];
+          typename Stage4<R>::type l{};  // low parts (FP32) and imaginary charges (complex); FP64 real: none
+          if constexpr (HILO || CPLX) l = sm.lo[j];
           Q q;
           if constexpr (CPLX) q = Q{h.w, l.w};
           else q = h.w;
@@ -855,7 +857,8 @@ __global__ void __launch_bounds__(128, XFMM_NEAR_MINB) k_near(NearArgs a) {
     else if (T <= 96 || XFMM_NEAR_MAXTPL == 3) near_leaf<KER, R, (XFMM_NEAR_MAXTPL >= 3 ? 3 : 1)>(a, node, lane, sm[wid]);
     else near_leaf<KER, R, (XFMM_NEAR_MAXTPL >= 4 ? 4 : 1)>(a, node, lane, sm[wid]);
   } else {
-    near_leaf<KER, R, 1>(a, node, lane, sm[wid]);  // FP64: one target per lane keeps occupancy up
+    // FP64: one target per lane keeps occupancy up (two per lane: 134 registers, 27.6 -> 31.3 ms at 4M)
+    near_leaf<KER, R, 1>(a, node, lane, sm[wid]);
   }
 }
 
