@@ -293,9 +293,11 @@ def roofline(r, peaks, src):
     tr_flops = 2 * 2.0 * (info["nnonleafs"]) * nsurf * 8 * nsurf  # M2M + L2L
     trans = {"pinv_fp64_tflops": pinv_flops / ((st["P2M"] + st["L2P_dc2e"]) * 1e-3) / 1e12,
              "m2m_l2l_fp32_tflops": tr_flops / ((st["M2M"] + st["L2L"]) * 1e-3) / 1e12,
-             "note": "library GEMMs: FP64 pinv factors on the FP64 tensor cores, truncated to the kept singular "
-                     "values; FP32 M2M/L2L as cuBLAS BF16x9 emulation on the tensor cores (FP32 accuracy); stage "
-                     "times include the row gather/scatter kernels and, for P2M, the check potentials"}
+             "note": "hand-written level-batched GEMMs with fused row gather, scale and scatter: FP64 pinv "
+                     "factors on the FP64 tensor cores (k_tgemm_f64, DMMA), truncated to the kept singular values; "
+                     "M2M/L2L and L2P's first factor as TF32x3 on tcgen05 with TMEM accumulators (k_tgemm_tc, FP32 "
+                     "accuracy); P2M's stage time includes its check potentials; tensor-pipe utilisation per "
+                     "kernel in profiles/translation_gemms_laplace_500k_p8_mixed.md"}
     return near, m2l, trans
 
 
