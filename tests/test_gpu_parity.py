@@ -209,6 +209,38 @@ def test_high_orders_against_direct_sums(kernel, p, wk):
     assert pm < 5e-6 and gm < 5e-6, (pm, gm)        # mixed precision against FP64 on the same tree
 
 
+# Orders past the own transform kernels (real p > 10, complex p > 12): the M2L runs on cuFFT over the
+# materialised convolution grids (k_m2l_grid_up, cuFFT R2C/C2C and the inverse, transposes to and from the
+# Hadamard's frequency-major layout), the per-level kernels with one plan pair per level.
+@pytest.mark.parametrize("kernel,p,wk", [("laplace", 12, 0.0), ("modified_helmholtz", 11, 5.0),
+                                         ("helmholtz", 13, 10.0 + 0.0j)])
+def test_cufft_fallback_orders_against_direct_sums(kernel, p, wk):
+    rng = np.random.default_rng(12)
+    n = 12000
+    x = rng.random((n, 3))
+    q = rng.uniform(-1, 1, n)
+    if kernel == "helmholtz":
+        q = q + 1j * rng.uniform(-1, 1, n)
+    m = _mod(kernel)
+    outs = {}
+    for prec in ("fp64", "mixed"):
+        if kernel == "laplace":
+            fmm = m.LaplaceFmm(p, 64, precision=prec)
+        elif kernel == "modified_helmholtz":
+            fmm = m.ModifiedHelmholtzFmm(p, 64, float(np.real(wk)), precision=prec)
+        else:
+            fmm = m.HelmholtzFmm(p, 64, complex(wk), precision=prec)
+        tree = m.setup(m.init_sources(x, q), m.init_targets(x), fmm)
+        outs[prec] = m.evaluate(tree, fmm)
+        fmm.stage_times(tree)  # raises if a bounded device-side wait ran out
+    s = rng.choice(n, 300, replace=False)
+    ex = orc.direct(kernel, x, q, x[s], wk) if kernel != "laplace" else orc.direct(kernel, x, q, x[s])
+    pe, ge = orc.rel_l2(outs["fp64"][s], ex)
+    assert pe < 1e-5 and ge < 1e-4, (pe, ge)         # the FMM's own truncation error at this order
+    pm, gm = orc.rel_l2(outs["mixed"], outs["fp64"])
+    assert pm < 5e-6 and gm < 5e-6, (pm, gm)        # mixed precision against FP64 on the same tree
+
+
 def test_sparse_hadamard_tile_option():
     """xfmm_set_tuning: the sparse Hadamard's tiles per CTA change the launch, not the result (beyond
     the mixed path's run-to-run rounding); out-of-range values are rejected."""
