@@ -313,10 +313,11 @@ __global__ void __launch_bounds__(TG_NT, 4) k_tgemm_tf32(int M, int N, int K, co
 // The same C = alpha A B as k_tgemm_tf32 on the sm_100 tensor cores.  A CTA owns 128 rows (one per TMEM
 // lane), 64 columns and a range of 16-wide K steps (K split over blockIdx.z when a level has few rows;
 // the parts are then added into C with atomics, C already holding the rows' starting values).
-// Per step: the rows' A pieces arrive raw by cp.async two steps ahead (16 bytes per lane, coalesced), are
-// split into TF32 head and tail one step ahead and stored into shared memory as K-major core matrices
-// (8 rows x 16 bytes, 128 contiguous bytes each); the operator's head and tail (pre-split, transposed to
-// [N][K], zero-padded to whole tiles) arrive by cp.async in the same layout, two steps ahead.  The proxy
+// Per step: the rows' A pieces arrive raw by cp.async two steps ahead (16 bytes per lane, coalesced), in
+// place into the stage's A-tail tile or into a raw buffer, and are split into TF32 head and tail one step
+// ahead as K-major core matrices (8 rows x 16 bytes, 128 contiguous bytes each); the operator's head and
+// tail (pre-split, transposed to [N][K], zero-padded to whole tiles) arrive by cp.async in the same
+// layout, two steps ahead.  The proxy
 // fence that hands a split step to the tensor core is issued before the next step's copies, so that it
 // has none of this thread's copies in flight to wait for (measured: 5% faster M2M and L2L).  One
 // elected lane of warp 0 issues the step's six MMAs (M128 N64 K8; Ah Bt + At Bh + Ah Bh per half step,
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(TG_NT, 4) k_tgemm_tf32(int M, int N, int K, co
 // accumulator's mbarrier.  While they run, every warp reads the previous step's accumulator back (its 32
 // lanes x 64 columns) and adds it to FP32 running sums with round-to-nearest adds.  Waits are bounded
 // (about a second); one that runs out sets the status flag and ends the loop.
-constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 16, TC_NT = 128, TC_ST = 3;
+constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 16, TC_NT = 128, TC_D = 2, TC_ST = TC_D + 1;
 #ifndef XFMM_TC_KSPLIT_MAX
 #define XFMM_TC_KSPLIT_MAX 64  // largest K split of a tensor-core translation GEMM
 #endif
@@ -334,7 +335,10 @@ constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 16, TC_NT = 128, TC_ST = 3;
 constexpr uint32_t TC_CORE = 128;                                         // bytes per core matrix
 constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK * 4, TC_B_BYTES = TC_BN * TC_BK * 4;
 constexpr uint32_t TC_STAGE = 2 * TC_A_BYTES + 2 * TC_B_BYTES;            // A head, A tail, B head, B tail
-constexpr size_t TC_SMEM = TC_ST * (size_t)TC_STAGE + 2 * (size_t)TC_A_BYTES + 1024;  // + 2 raw A buffers, alignment
+// shared memory: the stages (+ alignment), and for the raw-buffer form two raw A buffers
+constexpr size_t TC_SMEM_IP = TC_ST * (size_t)TC_STAGE + 1024;                    // in place: 3 CTAs per SM
+constexpr size_t TC_SMEM_RAW = TC_SMEM_IP + 2 * (size_t)TC_A_BYTES;             // raw buffers: 2 CTAs per SM
+template <bool IP> constexpr size_t tc_smem() { return IP ? TC_SMEM_IP : TC_SMEM_RAW; }
 constexpr long long TC_WAIT = 2000000000LL;
 
 // byte offset of element (row, k) (k < 16) in a K-major tile of 16-wide rows: core (row / 8, k / 4)
@@ -357,6 +361,13 @@ __device__ __forceinline__ void ld_32x32b_x64(uint32_t taddr, uint32_t (&v)[64])
                : "r"(taddr)
                : "memory");
 }
+// cp.async.wait_group with a run-time count (0..3 groups left in flight)
+__device__ __forceinline__ void cp_wait_dyn(int n) {
+  if (n <= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
+  else if (n == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
+  else if (n == 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
+  else asm volatile("cp.async.wait_group 3;" ::: "memory");
+}
 // Waits (spinning) for the phase of the given parity; false after `limit` SM clock cycles
 __device__ __forceinline__ bool mbar_spin(uint32_t mbar, uint32_t parity, long long limit) {
   if (tc5::mbar_try_wait(mbar, parity)) return true;
@@ -366,8 +377,8 @@ __device__ __forceinline__ bool mbar_spin(uint32_t mbar, uint32_t parity, long l
   return true;
 }
 
-template <class TC, int VA>
-__global__ void __launch_bounds__(TC_NT, 2)
+template <class TC, int VA, bool IP>
+__global__ void __launch_bounds__(TC_NT, IP ? 3 : 2)
     k_tgemm_tc(int M, int N, int K, const float* __restrict__ A, const int64_t* __restrict__ aoff,
                const float* __restrict__ Bth, const float* __restrict__ Btl, int64_t ldbt,
                const double* __restrict__ alpha, TC* __restrict__ C, const int64_t* __restrict__ coff, int acc,
@@ -378,7 +389,6 @@ __global__ void __launch_bounds__(TC_NT, 2)
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag;
   unsigned char* sm = tc_raw + ((1024 - (smem_u32(tc_raw) & 1023)) & 1023);  // stages on a 1 KB boundary
-  unsigned char* rawA = sm + TC_ST * (size_t)TC_STAGE;                        // 2 raw A buffers
   const uint32_t sm_u = smem_u32(sm);
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
@@ -411,10 +421,16 @@ __global__ void __launch_bounds__(TC_NT, 2)
   }
   const int kq = ((tid >> 3) & 3) * 4;
   // raw A pieces (zero-filled outside the rows and K) and the operator rows of step c (absolute index),
-  // one cp.async group
+  // one cp.async group.  In place (IP), a raw piece lands where its TF32 tail will be (the stage's
+  // A-tail tile, same core-matrix offset) and the thread that splits it writes the tail over it;
+  // otherwise it lands in the raw buffer of its step's parity.
+  unsigned char* rawA = sm + TC_ST * (size_t)TC_STAGE;
+  auto raw_piece = [&](unsigned char* st, int c, int q) -> unsigned char* {
+    if constexpr (IP) return st + TC_A_BYTES + tc_off(prow(q), kq);
+    else return rawA + (size_t)(c & 1) * TC_A_BYTES + (size_t)q * 16;
+  };
   auto fetch = [&](int c) {
     unsigned char* st = sm + (size_t)(c % TC_ST) * TC_STAGE;
-    unsigned char* ra = rawA + (size_t)(c & 1) * TC_A_BYTES;
     const int k0 = c * TC_BK;
 #pragma unroll
     for (int i = 0; i < 2; i++) {
@@ -431,7 +447,7 @@ __global__ void __launch_bounds__(TC_NT, 2)
     for (int i = 0; i < 4; i++) {
       const int k = k0 + kq;
       const int left = K - k;
-      const uint32_t dst = smem_u32(ra + (size_t)(tid + TC_NT * i) * 16);
+      const uint32_t dst = smem_u32(raw_piece(st, c, tid + TC_NT * i));
       const bool any = arow[i] >= 0 && left > 0;
       const float* src = any ? A + arow[i] + k : A;  // a chunk that reads nothing still names A
       if constexpr (VA == 16) {
@@ -450,11 +466,10 @@ __global__ void __launch_bounds__(TC_NT, 2)
   // this thread's raw pieces of step c (its own copies) split into the head and tail tiles of its stage
   auto split = [&](int c) {
     unsigned char* st = sm + (size_t)(c % TC_ST) * TC_STAGE;
-    const unsigned char* ra = rawA + (size_t)(c & 1) * TC_A_BYTES;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const int q = tid + TC_NT * i;
-      const float4 v = *reinterpret_cast<const float4*>(ra + (size_t)q * 16);
+      const float4 v = *reinterpret_cast<const float4*>(raw_piece(st, c, q));
       uint32_t h[4], l[4];
       split_tf32(v.x, h[0], l[0]);
       split_tf32(v.y, h[1], l[1]);
@@ -482,12 +497,13 @@ __global__ void __launch_bounds__(TC_NT, 2)
     for (int j = 0; j < TC_BN; j++) run[j] = __fadd_rn(run[j], __uint_as_float(v[j]));
   };
   constexpr uint32_t IDESC = idesc_tf32(TC_BM, TC_BN);
-  // prologue: steps 0 and 1 fetched, step 0 split
-  if (nc > 0) fetch(c0);
-  if (nc > 1) fetch(c0 + 1);
-  if (nc > 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
-  else asm volatile("cp.async.wait_group 0;" ::: "memory");
-  if (nc > 0) split(c0);
+  // prologue: steps 0 .. TC_D - 1 fetched, step 0 split
+  for (int j = 0; j < TC_D; j++)
+    if (j < nc) fetch(c0 + j);
+  if (nc > 0) {
+    cp_wait_dyn(min(TC_D, nc) - 1);
+    split(c0);
+  }
   barrier();
   bool ok = true;
   for (int i = 0; i < nc && ok; i++) {
@@ -521,14 +537,14 @@ __global__ void __launch_bounds__(TC_NT, 2)
         if (lane == 0) abort_flag = 1;
       }
     }
-    // step c + 1 is split and made visible to the tensor core (proxy fence) before step c + 2's copies are
-    // issued, so that the fence has no copies of this thread in flight to wait for
+    // step c + 1 is split and made visible to the tensor core (proxy fence) before step c + TC_D's copies
+    // are issued (copies of steps c + 1 .. c + TC_D - 1 are in flight; step c + 1's must have landed)
     if (ok && i + 1 < nc) {
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      cp_wait_dyn(min(TC_D - 2, nc - 2 - i));
       split(c + 1);
     }
     fence_proxy_async_smem();
-    if (ok && i + 2 < nc) fetch(c + 2);  // into the stage of step c - 1 and the raw buffer of step c
+    if (ok && i + TC_D < nc) fetch(c + TC_D);  // into the stage of step c - 1
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
@@ -708,13 +724,17 @@ void tgemm_tc(const TGemm& g, const float* A, const float* Bth, const float* Btl
              "split tensor-core translation: scratch too small");
   }
   const dim3 grid(mt, nt, kz);
-  auto go = [&](auto kern) {
-    XCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-    kern<<<grid, TC_NT, TC_SMEM, s>>>(g.M, g.N, g.K, A, g.aoff, Bth, Btl, ldbt, g.alpha, C, g.coff, g.accumulate,
-                                      g.status, g.scratch);
+  // In place, three CTAs share an SM; measured faster except for short K (fewer than 32 steps) with many
+  // column tiles (the Laplace L2L: 0.86 ms with the raw buffers, 1.06 ms in place), which keeps the raw
+  // buffers and two CTAs per SM.
+  const bool ip = !(nsteps < 32 && nt >= 16);
+  auto go = [&](auto kern, size_t smem) {
+    XCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, TC_NT, smem, s>>>(g.M, g.N, g.K, A, g.aoff, Bth, Btl, ldbt, g.alpha, C, g.coff, g.accumulate,
+                                   g.status, g.scratch);
   };
-  if (g.astep % 4 == 0) go(k_tgemm_tc<TC, 16>);
-  else go(k_tgemm_tc<TC, 8>);
+  if (g.astep % 4 == 0) ip ? go(k_tgemm_tc<TC, 16, true>, TC_SMEM_IP) : go(k_tgemm_tc<TC, 16, false>, TC_SMEM_RAW);
+  else ip ? go(k_tgemm_tc<TC, 8, true>, TC_SMEM_IP) : go(k_tgemm_tc<TC, 8, false>, TC_SMEM_RAW);
   XLAUNCH();
   if (kz > 1) {
     k_tc_finish<TC><<<tg_blocks((int64_t)g.M * g.N), 256, 0, s>>>(g.M, g.N, g.scratch, C, g.coff, g.accumulate);
