@@ -1266,29 +1266,15 @@ __device__ __forceinline__ void hadt_tile(const float4& x0, const float4& x1, co
 
 // Round form on the tensor cores (sparse targets): each round of 64 same-position pairs as 4 row tiles of
 // 16 (pair 16 j + g and 16 j + 8 + g of tile j); lanes t and t ^ 1 trade halves so each adds 16 bytes
-// (two target components of one pair) with a vector atomic.
-__global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 registers, a 16-byte spill)
-    k_hadamard_rt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
-                  const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
-                  const int* __restrict__ rows, int ntiles, int tpc, int nsrc, int ntrg, int nfreq) {
+// (two target components of one pair) with a vector atomic.  Rounds [r0, r1) at one frequency: warp wid
+// takes every (HADR_NT / 32)-th round; inf points at the frequency's spectra (+ lane quad offset t), of at
+// its product rows, and the rows were zeroed by the same CTA.
+__device__ __forceinline__ void hadr_rounds(const uint4* sB, const float4* __restrict__ inf, float2* of,
+                                            const int* __restrict__ rpos, const int2* __restrict__ ent, int r0,
+                                            int r1, int wid, int lane) {
   constexpr int NW = HADR_NT / 32;
   static_assert(HADR_RW == 64, "a round is 4 row tiles of 16 pairs");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint4* sB = reinterpret_cast<uint4*>(smem_raw);
-  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  // tiles [tb, te) share this CTA's B fragments of frequency f
-  const int tb = blockIdx.x * tpc, te = min(ntiles, tb + tpc);
-  float2* of = out + (int64_t)f * ntrg * 8;
-  // every product of these tiles' targets at frequency f is added by this CTA: their rows start at zero
-  for (int e = tid; e < (te - tb) * HADR_TT * 4; e += HADR_NT) {
-    const int row = rows[tb * HADR_TT + (e >> 2)];
-    if (row >= 0) reinterpret_cast<float4*>(of + (int64_t)row * 8)[e & 3] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  hadt_fill_b(sB, T, f, nfreq, tid, HADR_NT);
-  __syncthreads();
-  const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + t;
-  const int r1 = tile_r[te];
   // a round's pairs (source, output row) and their spectra, all loads in flight at once
   auto load_round = [&](int r, int2 (&ee)[4][2], float4 (&xx)[4][2]) {
 #pragma unroll
@@ -1301,7 +1287,7 @@ __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 
       for (int rr = 0; rr < 2; rr++)
         xx[j][rr] = ee[j][rr].x >= 0 ? __ldg(inf + (int64_t)ee[j][rr].x * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
   };
-  for (int r = tile_r[tb] + wid; r < r1; r += NW) {
+  for (int r = r0 + wid; r < r1; r += NW) {
     const int ipos = rpos[r];
     uint4 b[4];
 #pragma unroll
@@ -1324,6 +1310,67 @@ __global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 
         if (e.x >= 0) atomicAdd(reinterpret_cast<float4*>(of + (int64_t)e.y * 8 + 4 * h + (t & ~1)), v);
       }
     }
+  }
+}
+
+__global__ void __launch_bounds__(HADR_NT, 3)  // 3 blocks/SM measured best (80 registers, a 16-byte spill)
+    k_hadamard_rt(const float2* __restrict__ T, const float2* __restrict__ in, float2* __restrict__ out,
+                  const int* __restrict__ tile_r, const int* __restrict__ rpos, const int2* __restrict__ ent,
+                  const int* __restrict__ rows, int ntiles, int tpc, int nsrc, int ntrg, int nfreq) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint4* sB = reinterpret_cast<uint4*>(smem_raw);
+  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  // tiles [tb, te) share this CTA's B fragments of frequency f
+  const int tb = blockIdx.x * tpc, te = min(ntiles, tb + tpc);
+  float2* of = out + (int64_t)f * ntrg * 8;
+  // every product of these tiles' targets at frequency f is added by this CTA: their rows start at zero
+  for (int e = tid; e < (te - tb) * HADR_TT * 4; e += HADR_NT) {
+    const int row = rows[tb * HADR_TT + (e >> 2)];
+    if (row >= 0) reinterpret_cast<float4*>(of + (int64_t)row * 8)[e & 3] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  hadt_fill_b(sB, T, f, nfreq, tid, HADR_NT);
+  __syncthreads();
+  const float4* inf = reinterpret_cast<const float4*>(in + (int64_t)f * nsrc * 8) + (lane & 3);
+  hadr_rounds(sB, inf, of, rpos, ent, tile_r[tb], tile_r[te], wid, lane);
+}
+
+// The round form over the sparse tiles of many systems that share one operator table (a batch of Laplace
+// systems): tiles[k] = (system, its tile), and a CTA covers tiles [tb, te) of the list, possibly of several
+// systems, with one B fill per frequency.
+struct HadSys {
+  const float2* in;     // spectra [f][source][child]
+  float2* out;          // products [f][target][child]
+  const int* tile_r;    // rounds of each sparse tile (CSR)
+  const int* rpos;      // relative position of each round
+  const int2* ent;      // pairs of each round
+  const int* rows;      // HADR_TT output rows per tile
+  int nsrc, ntrg;
+};
+__global__ void __launch_bounds__(HADR_NT, 3)
+    k_hadamard_rt_batch(const float2* __restrict__ T, const HadSys* __restrict__ sys, const int2* __restrict__ tiles,
+                        int ntiles, int tpc, int nfreq) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint4* sB = reinterpret_cast<uint4*>(smem_raw);
+  const int f = blockIdx.y, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tb = blockIdx.x * tpc, te = min(ntiles, tb + tpc);
+  for (int k = tb; k < te; k++) {
+    const int2 tl = tiles[k];
+    const HadSys& S = sys[tl.x];
+    float2* of = S.out + (int64_t)f * S.ntrg * 8;
+    const int* rows = S.rows + (int64_t)tl.y * HADR_TT;
+    for (int e = tid; e < HADR_TT * 4; e += HADR_NT) {
+      const int row = rows[e >> 2];
+      if (row >= 0) reinterpret_cast<float4*>(of + (int64_t)row * 8)[e & 3] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  hadt_fill_b(sB, T, f, nfreq, tid, HADR_NT);
+  __syncthreads();
+  for (int k = tb; k < te; k++) {
+    const int2 tl = tiles[k];
+    const HadSys& S = sys[tl.x];
+    const float4* inf = reinterpret_cast<const float4*>(S.in + (int64_t)f * S.nsrc * 8) + (lane & 3);
+    hadr_rounds(sB, inf, S.out + (int64_t)f * S.ntrg * 8, S.rpos, S.ent, S.tile_r[tl.y], S.tile_r[tl.y + 1], wid,
+                lane);
   }
 }
 
@@ -2618,6 +2665,7 @@ void find_close_pairs(Workspace& ws, const NearArgs& na, int n_eval, cudaStream_
 }
 
 constexpr int DOWN_PRE = 1, DOWN_NEAR = 2, DOWN_FAR = 4, DOWN_ALL = 7;
+constexpr int M2L_FWD = 1, M2L_HAD_SPARSE = 2, M2L_HAD_DENSE = 4, M2L_BWD = 8, M2L_ALL = 15;
 
 // ------------------------------------------------------------------ engine, per kernel and precision
 template <int KER, class R>
@@ -2684,7 +2732,8 @@ struct Engine {
     XCUDA(cudaEventRecord(ws.ev[2], s));
   }
 
-  static void m2l(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s) {
+  // phase: which parts of every group's M2L to run (M2L_FWD, M2L_HAD_SPARSE, M2L_HAD_DENSE, M2L_BWD)
+  static void m2l(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int phase = M2L_ALL) {
     const int n = f.nsurf, nconv = f.nconv, nfreq = f.nfreq;
     const int ng = (int)t.m2l_src_off.size() - 1;
     for (int g = 0; g < ng; g++) {
@@ -2695,6 +2744,7 @@ struct Engine {
       const int* trg = t.m2l_trg.p + t.m2l_trg_off[g];
       const int tab_level = KER == K_LAPLACE ? 0 : g + 1;
       const CT* T = (const CT*)f.ops[tab_level].m2l_T.p;
+      if (phase & M2L_FWD) {
       XCUDA(cudaEventRecord(ev[0], s));
       // upward equivalent DFT (fmm_scale_invariant.h:560-604) -> specB [f][s][c]
       if constexpr (KER != K_HELMHOLTZ) {
@@ -2737,11 +2787,13 @@ struct Engine {
         transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, (int64_t)ns * 8, nfreq, s);  // -> [f][s][c]
       }
       XCUDA(cudaEventRecord(ev[1], s));
+      }
+      if (phase & (M2L_HAD_SPARSE | M2L_HAD_DENSE)) {
       // Hadamard product
       const int ntiles = ws.had_tile0[g + 1] - ws.had_tile0[g];
       if constexpr (sizeof(CT) == 8) {
         XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
-        if (ntiles > 0) {
+        if (ntiles > 0 && (phase & M2L_HAD_SPARSE)) {
           const int* rows = ws.hadr_row.p + (int64_t)ws.had_tile0[g] * HADR_TT;
           if (!ws.hadrt_attr) {
             XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
@@ -2754,7 +2806,7 @@ struct Engine {
           XLAUNCH();
           ws.launches++;
         }
-        if (ws.hadd_ld[g] > 0 && ws.had_tc5) {
+        if (ws.hadd_ld[g] > 0 && ws.had_tc5 && (phase & M2L_HAD_DENSE)) {
           if (!ws.hadc_attr) {
             XCUDA(cudaFuncSetAttribute(k_hadamard_dc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADC_SMEM));
             ws.hadc_attr = true;
@@ -2773,7 +2825,7 @@ struct Engine {
               ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq, ws.status.p);
           XLAUNCH();
           ws.launches++;
-        } else if (ws.hadd_ld[g] > 0) {
+        } else if (ws.hadd_ld[g] > 0 && (phase & M2L_HAD_DENSE)) {
           if (!ws.hadt_attr) {
             XCUDA(cudaFuncSetAttribute(k_hadamard_dt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
             ws.hadt_attr = true;
@@ -2786,7 +2838,7 @@ struct Engine {
         }
       } else {
         XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
-        if (ws.hadd_ld[g] > 0) {
+        if (ws.hadd_ld[g] > 0 && (phase & M2L_HAD_DENSE)) {
           if (!ws.had64_attr) {
             XCUDA(cudaFuncSetAttribute(k_hadamard_d64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HAD64_SMEM));
             ws.had64_attr = true;
@@ -2799,6 +2851,8 @@ struct Engine {
         }
       }
       XCUDA(cudaEventRecord(ev[2], s));
+      }
+      if (phase & M2L_BWD) {
       // inverse DFT of specA [f][t][c] to the downward check potentials (fmm_scale_invariant.h:606-646)
       if constexpr (KER != K_HELMHOLTZ) {
         if (ws.fused) {
@@ -2854,6 +2908,7 @@ struct Engine {
         ws.launches += 2;
       }
       XCUDA(cudaEventRecord(ev[3], s));
+      }
     }
   }
 
@@ -2884,9 +2939,9 @@ struct Engine {
 
   // phases: DOWN_PRE (P2L, M2L, L2L, L2P check-to-equivalent), DOWN_NEAR (P2P), DOWN_FAR (M2P + L2P
   // evaluation, added to the near field's values); an evaluate runs all three in this order
-  static void downward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int phases = DOWN_ALL) {
+  static void downward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int phases = DOWN_ALL, int m2l_phase = M2L_ALL) {
     const int n = f.nsurf;
-    if (phases & DOWN_PRE) downward_pre(f, t, ws, s);
+    if (phases & DOWN_PRE) downward_pre(f, t, ws, s, m2l_phase);
     if (t.n_eval_leafs && (phases & DOWN_NEAR)) {
       NearArgs na = near_args(f, t, ws);
       if constexpr (KER == K_LAPLACE && sizeof(R) == 4) {
@@ -2924,10 +2979,12 @@ struct Engine {
     if (phases & DOWN_FAR) XCUDA(cudaEventRecord(ws.ev[7], s));
   }
 
-  static void downward_pre(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s) {
+  // m2l_phase: the parts of the M2L to run (M2L_ALL for an evaluate); P2L runs with the forward transforms,
+  // L2L and L2P's check-to-equivalent step with the backward ones
+  static void downward_pre(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int m2l_phase = M2L_ALL) {
     const int n = f.nsurf;
     // P2L (X list) into downward check potentials
-    if (t.n_p2l_nodes) {
+    if (t.n_p2l_nodes && (m2l_phase & M2L_FWD)) {
       SurfPotArgs a{t.p2l_nodes.p, t.n_p2l_nodes, t.nsrcs.p,     t.p2l.p, t.level.p, t.sbeg.p, t.p2l_off.p, t.center.p,
                     t.src4.p,      t.src_qim.p,   f.surf_base.p, n,       1.05,      ws.dn.p,  1,           f.k_re,
                     f.k_im,        INV4PI * op_scale(f, t)};
@@ -2935,9 +2992,10 @@ struct Engine {
       XLAUNCH();
       ws.launches++;
     }
-    XCUDA(cudaEventRecord(ws.ev[3], s));
+    if (m2l_phase & M2L_FWD) XCUDA(cudaEventRecord(ws.ev[3], s));
     // M2L
-    if (t.n_m2l_trg) m2l(f, t, ws, s);
+    if (t.n_m2l_trg) m2l(f, t, ws, s, m2l_phase);
+    if (!(m2l_phase & M2L_BWD)) return;
     XCUDA(cudaEventRecord(ws.ev[4], s));
     // L2L: shallowest parents first (pre-order); per level one GEMM of the parents' rows with the
     // [n][8n] operator, added to the 8 children rows (contiguous per parent)
@@ -3128,6 +3186,12 @@ struct Batch {
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;
   int near_ctas_per_sm = 0, near_tpl = 2;  // tuning (0: the kernel's resident limit)
+  // mixed Laplace systems sharing one operator table: the sparse M2L Hadamard of every system in one launch
+  bool had_batched = false;
+  const float2* had_T = nullptr;
+  int had_nfreq = 0, had_tpc = HADR_TPC, nhtiles = 0;
+  DBuf<HadSys> hsys;
+  DBuf<int2> htiles;
   ~Batch() {
     for (auto e : events) cudaEventDestroy(e);
     for (auto st : streams) cudaStreamDestroy(st);
@@ -3186,6 +3250,38 @@ Batch* batch_create(Fmm** fmms, Tree** trees, int n, cudaStream_t s) {
         off += ws.n_close;
       }
     }
+    // one operator table for every system (one Fmm), mixed Laplace (one M2L group): the sparse Hadamard
+    // tiles of all systems as one list
+    bool shared = b->kernel == XFMM_LAPLACE && b->precision == XFMM_MIXED;
+    for (int k = 1; k < n && shared; k++) shared = fmms[k] == fmms[0];
+    if (shared) {
+      std::vector<HadSys> hs(n);
+      std::vector<int2> tl;
+      for (int k = 0; k < n; k++) {
+        Tree& t = *trees[k];
+        Workspace& ws = *t.ws[fmms[k]->precision];
+        HadSys& h = hs[k];
+        h = HadSys{};
+        if (t.n_m2l_trg == 0 || t.m2l_src_off.size() != 2) continue;
+        h.in = (const float2*)ws.specB.p;
+        h.out = (float2*)ws.specA.p;
+        h.tile_r = ws.hadr_tile.p + ws.had_tile0[0];
+        h.rpos = ws.hadr_pos.p;
+        h.ent = ws.hadr_ent.p;
+        h.rows = ws.hadr_row.p + (int64_t)ws.had_tile0[0] * HADR_TT;
+        h.nsrc = t.m2l_src_off[1] - t.m2l_src_off[0];
+        h.ntrg = t.m2l_trg_off[1] - t.m2l_trg_off[0];
+        for (int j = 0; j < ws.had_tile0[1] - ws.had_tile0[0]; j++) tl.push_back(make_int2(k, j));
+      }
+      b->had_batched = true;
+      b->had_T = (const float2*)fmms[0]->ops[0].m2l_T.p;
+      b->had_nfreq = fmms[0]->nfreq;
+      b->nhtiles = (int)tl.size();
+      b->hsys.upload(hs, s);
+      if (!tl.empty()) b->htiles.upload(tl, s);
+      XREQUIRE(b->had_nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
+      XCUDA(cudaFuncSetAttribute(k_hadamard_rt_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
+    }
     b->order.resize(n);
     for (int k = 0; k < n; k++) b->order[k] = k;
     std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return bodies[x] > bodies[y]; });
@@ -3219,6 +3315,9 @@ void batch_set_tuning(Batch* b, int option, int value) {
   } else if (option == XFMM_BATCH_NEAR_TARGETS_PER_LANE) {
     XREQUIRE(value == 1 || value == 2, XFMM_ERR_ARG, "targets per lane must be 1 or 2");
     b->near_tpl = value;
+  } else if (option == XFMM_BATCH_HADAMARD_TILES_PER_CTA) {
+    XREQUIRE(value >= 0 && value <= 64, XFMM_ERR_ARG, "Hadamard tiles per CTA must be 0..64");
+    b->had_tpc = value > 0 ? value : HADR_TPC;
   } else {
     XREQUIRE(false, XFMM_ERR_ARG, "unknown batch tuning option");
   }
@@ -3236,7 +3335,7 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
     XCUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     b->streams.push_back(st);
   }
-  while (b->events.size() < (size_t)2 * (nstreams + 1)) {
+  while (b->events.size() < (size_t)3 * (nstreams + 1)) {
     cudaEvent_t e;
     XCUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     b->events.push_back(e);
@@ -3260,6 +3359,9 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
       XCUDA(cudaStreamWaitEvent(s, b->events[evbase + 1 + j], 0));
     }
   };
+  // before the near field: upward pass, P2L, M2L and L2L per system; with one shared operator table the
+  // sparse M2L Hadamard of every system runs as one launch between the forward and backward transforms
+  const int pre1 = b->had_batched ? (M2L_FWD | M2L_HAD_DENSE) : M2L_ALL;
   fork_join(0, [&](int k, cudaStream_t st) {
     Fmm& f = *b->fmm[k];
     Tree& t = *b->tree[k];
@@ -3268,9 +3370,23 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
     Workspace& ws = workspace(f, t, st);
     dispatch(f, [&](auto e) {
       decltype(e)::upward(f, t, ws, st);
-      decltype(e)::downward(f, t, ws, st, DOWN_PRE);
+      decltype(e)::downward(f, t, ws, st, DOWN_PRE, pre1);
     });
   });
+  if (b->had_batched) {
+    if (b->nhtiles > 0) {
+      const int tpc = std::max(1, b->had_tpc);
+      k_hadamard_rt_batch<<<dim3((b->nhtiles + tpc - 1) / tpc, b->had_nfreq), HADR_NT, HADT_SMEM, s>>>(
+          b->had_T, b->hsys.p, b->htiles.p, b->nhtiles, tpc, b->had_nfreq);
+      XLAUNCH();
+    }
+    fork_join(2 * (nstreams + 1), [&](int k, cudaStream_t st) {
+      Fmm& f = *b->fmm[k];
+      Tree& t = *b->tree[k];
+      Workspace& ws = workspace(f, t, st);
+      dispatch(f, [&](auto e) { decltype(e)::downward(f, t, ws, st, DOWN_PRE, M2L_BWD); });
+    });
+  }
   // the near field of every system: one persistent launch draining the work queue
   if (b->nitems > 0) {
     int dev = 0, nsm = 148;

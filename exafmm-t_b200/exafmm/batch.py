@@ -4,7 +4,9 @@ reference, which evaluates one system per call).
 Each system gets its own tree, lists and device buffers for its charges and results.  Laplace systems
 share one Fmm object: its scale-invariant operators, precomputed once for the first system's root radius,
 serve every other radius (the evaluate scales the body-to-check potentials by the ratio of the radii);
-the other kernels' operators depend on the radius, so each of those systems gets its own Fmm object.  The systems are held by one native batch (xfmm_batch_*):
+the other kernels' operators depend on the radius, so each of those systems gets its own Fmm object.
+With one shared operator table (mixed Laplace) the sparse M2L Hadamard of every system is also one
+launch, between the systems' forward and backward M2L transforms.  The systems are held by one native batch (xfmm_batch_*):
 one evaluate of every system runs each system's stages before and after its near field on concurrent
 streams forked from the batch stream (largest systems first, each to the least-loaded stream), and the
 near field of all systems as one persistent kernel that drains a work queue of (system, target leaf)
@@ -27,7 +29,7 @@ import torch
 
 from . import _core, _lib
 
-NEAR_CTAS_PER_SM, NEAR_TARGETS_PER_LANE = 1, 2  # include/xfmm.h XFMM_BATCH_NEAR_*
+NEAR_CTAS_PER_SM, NEAR_TARGETS_PER_LANE, HADAMARD_TILES_PER_CTA = 1, 2, 3  # include/xfmm.h XFMM_BATCH_*
 
 
 class BatchedFmm:
@@ -76,10 +78,14 @@ class BatchedFmm:
 
     def __del__(self):
         b = getattr(self, "_b", None)
-        if b is not None and b.value:
-            self.graph = None
+        if b is None or not b.value:
+            return
+        self.graph = None
+        self._b = None
+        try:
             _lib.lib().xfmm_batch_free(b)
-            self._b = None
+        except (AttributeError, TypeError):  # interpreter shutdown: the library module is already gone
+            pass
 
     def set_near_shape(self, ctas_per_sm, targets_per_lane):
         """Tile shape of the persistent near-field kernel; recapture after."""
@@ -139,9 +145,11 @@ class BatchedFmm:
         return e0.elapsed_time(e1) / reps
 
     def set_tiles_per_cta(self, value):
-        """Sparse M2L Hadamard tiles per CTA on every tree (0: the library default); recapture after."""
+        """Sparse M2L Hadamard tiles per CTA (0: the library default) of the batch's one-launch Hadamard
+        (systems sharing one operator set) and of every tree's own; recapture after."""
         for tree in self.trees:
             tree.set_tuning("sparse_hadamard_tiles_per_cta", value)
+        _lib.check(_lib.lib().xfmm_batch_set_tuning(self._b, HADAMARD_TILES_PER_CTA, int(value)))
         self.tiles_per_cta = int(value)
 
     def autotune(self, candidates=(4, 8, 16, 32), near_shapes=((0, 2), (4, 2), (0, 1), (2, 2)), reps=3,

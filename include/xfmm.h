@@ -146,14 +146,19 @@ xfmm_status xfmm_set_tuning(xfmm_tree* tree, int option, int value);
  * order) out.  Each system's stages before and after its near field run on `nstreams` concurrent streams
  * forked from `stream` (largest systems first, each to the least-loaded stream); the near field of all
  * systems is one persistent kernel draining a work queue of (system, target leaf) items, largest first,
- * and the exact close-pair corrections of all systems one more launch.  Asynchronous on `stream`, no
+ * and the exact close-pair corrections of all systems one more launch.  When every system uses the same
+ * xfmm_fmm handle, mixed Laplace with one scale-invariant operator set, the sparse M2L Hadamard of all
+ * systems is also one launch, between the systems' forward and backward M2L transforms.  Asynchronous on `stream`, no
  * allocation: it may be captured into a CUDA graph (after one evaluate outside the capture). */
 typedef struct xfmm_batch xfmm_batch;
 enum {
   /* persistent near field: CTAs per SM (0: as many as fit; 1..32) */
   XFMM_BATCH_NEAR_CTAS_PER_SM = 1,
   /* persistent near field: most targets a lane holds, the height of a warp's target tile (1 or 2) */
-  XFMM_BATCH_NEAR_TARGETS_PER_LANE = 2
+  XFMM_BATCH_NEAR_TARGETS_PER_LANE = 2,
+  /* one-launch sparse M2L Hadamard of mixed Laplace systems sharing one xfmm_fmm: 512-target tiles per CTA,
+   * which share one operator fill per frequency and may belong to different systems (1..64; 0: 4) */
+  XFMM_BATCH_HADAMARD_TILES_PER_CTA = 3
 };
 xfmm_status xfmm_batch_create(xfmm_fmm* const* fmms, xfmm_tree* const* trees, int n, void* stream, xfmm_batch** out);
 xfmm_status xfmm_batch_evaluate(xfmm_batch* batch, const double* const* charges, double* const* outs, int nstreams,
