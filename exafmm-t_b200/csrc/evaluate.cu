@@ -2666,6 +2666,11 @@ void find_close_pairs(Workspace& ws, const NearArgs& na, int n_eval, cudaStream_
 
 constexpr int DOWN_PRE = 1, DOWN_NEAR = 2, DOWN_FAR = 4, DOWN_ALL = 7;
 constexpr int M2L_FWD = 1, M2L_HAD_SPARSE = 2, M2L_HAD_DENSE = 4, M2L_BWD = 8, M2L_ALL = 15;
+// parts of the downward pass before the near field: the M2L parts above (P2L with the forward transforms),
+// then L2L, then L2P's check-to-equivalent step
+constexpr int PRE_L2L = 16, PRE_DC2E = 32, PRE_ALL = M2L_ALL | PRE_L2L | PRE_DC2E;
+// parts of the upward pass
+constexpr int UP_P2M = 1, UP_M2M = 2, UP_ALL = 3;
 
 // ------------------------------------------------------------------ engine, per kernel and precision
 template <int KER, class R>
@@ -2675,8 +2680,9 @@ struct Engine {
   using CT = typename C2<R>::type;              // spectrum value
   static constexpr int CW = KER == K_HELMHOLTZ ? 2 : 1;  // reals per value
 
-  static void upward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s) {
+  static void upward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int parts = UP_ALL) {
     const int n = f.nsurf;
+    if (parts & UP_P2M) {
     ws.launches = 0;
     XCUDA(cudaEventRecord(ws.ev[0], s));
     // P2M: check potentials of every leaf, then the pinv (UC2E) GEMM per leaf level
@@ -2711,6 +2717,8 @@ struct Engine {
       }
     }
     XCUDA(cudaEventRecord(ws.ev[1], s));
+    }
+    if (!(parts & UP_M2M)) return;
     // M2M: deepest parents first (post-order); per level one GEMM of the parents' 8 children rows
     // (contiguous per parent) with the [8n][n] operator, written to the parents' rows
     for (int l = t.depth - 1; l >= 0; l--) {
@@ -2939,7 +2947,7 @@ struct Engine {
 
   // phases: DOWN_PRE (P2L, M2L, L2L, L2P check-to-equivalent), DOWN_NEAR (P2P), DOWN_FAR (M2P + L2P
   // evaluation, added to the near field's values); an evaluate runs all three in this order
-  static void downward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int phases = DOWN_ALL, int m2l_phase = M2L_ALL) {
+  static void downward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int phases = DOWN_ALL, int m2l_phase = PRE_ALL) {
     const int n = f.nsurf;
     if (phases & DOWN_PRE) downward_pre(f, t, ws, s, m2l_phase);
     if (t.n_eval_leafs && (phases & DOWN_NEAR)) {
@@ -2979,9 +2987,9 @@ struct Engine {
     if (phases & DOWN_FAR) XCUDA(cudaEventRecord(ws.ev[7], s));
   }
 
-  // m2l_phase: the parts of the M2L to run (M2L_ALL for an evaluate); P2L runs with the forward transforms,
-  // L2L and L2P's check-to-equivalent step with the backward ones
-  static void downward_pre(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int m2l_phase = M2L_ALL) {
+  // m2l_phase: the parts to run (PRE_ALL for an evaluate): the M2L parts (P2L with the forward transforms),
+  // L2L (PRE_L2L) and L2P's check-to-equivalent step (PRE_DC2E)
+  static void downward_pre(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int m2l_phase = PRE_ALL) {
     const int n = f.nsurf;
     // P2L (X list) into downward check potentials
     if (t.n_p2l_nodes && (m2l_phase & M2L_FWD)) {
@@ -2995,8 +3003,8 @@ struct Engine {
     if (m2l_phase & M2L_FWD) XCUDA(cudaEventRecord(ws.ev[3], s));
     // M2L
     if (t.n_m2l_trg) m2l(f, t, ws, s, m2l_phase);
-    if (!(m2l_phase & M2L_BWD)) return;
-    XCUDA(cudaEventRecord(ws.ev[4], s));
+    if (m2l_phase & M2L_BWD) XCUDA(cudaEventRecord(ws.ev[4], s));
+    if (m2l_phase & PRE_L2L) {
     // L2L: shallowest parents first (pre-order); per level one GEMM of the parents' rows with the
     // [n][8n] operator, added to the 8 children rows (contiguous per parent)
     for (int l = 0; l < t.depth; l++) {
@@ -3014,6 +3022,8 @@ struct Engine {
       ws.launches++;
     }
     XCUDA(cudaEventRecord(ws.ev[5], s));
+    }
+    if (!(m2l_phase & PRE_DC2E)) return;
     // L2P part 1: downward check -> equivalent (DC2E) per leaf level, e = conj(U) S+ (conj(VH) 0.5^l c):
     // y over the kept singular directions, then e to the leaf positions (FP64).
     if (t.nleafs) {
@@ -3192,6 +3202,10 @@ struct Batch {
   int had_nfreq = 0, had_tpc = HADR_TPC, nhtiles = 0;
   DBuf<HadSys> hsys;
   DBuf<int2> htiles;
+  // with the shared table also the M2M and L2L of every system, per level one GEMM over all systems' rows
+  std::vector<GemmRows> bm2m, bl2l;  // row offsets rebased onto system 0's up / dn arrays
+  DBuf<double> bscratch;             // FP64 scratch of their split K (zero between uses)
+  int* bstatus = nullptr;            // system 0's device status flag (bounded waits)
   ~Batch() {
     for (auto e : events) cudaEventDestroy(e);
     for (auto st : streams) cudaStreamDestroy(st);
@@ -3273,6 +3287,51 @@ Batch* batch_create(Fmm** fmms, Tree** trees, int n, cudaStream_t s) {
         h.ntrg = t.m2l_trg_off[1] - t.m2l_trg_off[0];
         for (int j = 0; j < ws.had_tile0[1] - ws.had_tile0[0]; j++) tl.push_back(make_int2(k, j));
       }
+      // per-level translations over all systems' rows: offsets rebased onto system 0's up / dn arrays (every
+      // system's arrays are separate allocations, 256-byte aligned: the rebased offsets keep 16-byte rows)
+      int maxd = 0;
+      for (int k = 0; k < n; k++) maxd = std::max(maxd, trees[k]->depth);
+      const int prec = fmms[0]->precision, ns = fmms[0]->nsurf;
+      Workspace& w0 = *trees[0]->ws[prec];
+      const float* up0 = (const float*)w0.up.p;
+      const float* dn0 = (const float*)w0.dn.p;
+      b->bm2m.resize(maxd);
+      b->bl2l.resize(maxd);
+      int64_t need = 0;
+      for (int l = 0; l < maxd; l++) {
+        std::vector<int64_t> ma, mc, la, lc;
+        for (int k = 0; k < n; k++) {
+          Tree& t = *trees[k];
+          Workspace& ws = *t.ws[prec];
+          if (l >= t.depth) continue;
+          const int64_t du = (const float*)ws.up.p - up0, dd = (const float*)ws.dn.p - dn0;
+          const GemmRows& gm = ws.m2m[l];
+          const GemmRows& gl = ws.l2l[l];
+          if (gm.M > 0) {
+            const std::vector<int64_t> a = gm.a.download(s, (size_t)gm.M), c = gm.c.download(s, (size_t)gm.M);
+            for (int i = 0; i < gm.M; i++) {
+              ma.push_back(a[i] + du);
+              mc.push_back(c[i] + du);
+            }
+          }
+          if (gl.M > 0) {
+            const std::vector<int64_t> a = gl.a.download(s, (size_t)gl.M), c = gl.c.download(s, (size_t)gl.M);
+            for (int i = 0; i < gl.M; i++) {
+              la.push_back(a[i] + dd);
+              lc.push_back(c[i] + dd);
+            }
+          }
+        }
+        upload_rows<double>(b->bm2m[l], ma, mc, std::vector<double>(ma.size(), 1.0), s);
+        upload_rows<double>(b->bl2l[l], la, lc, std::vector<double>(la.size(), 1.0), s);
+        need = std::max(need, tgemm_tc_scratch((int)ma.size(), ns, 8 * ns, 1));
+        need = std::max(need, tgemm_tc_scratch((int)la.size(), 8 * ns, ns, 1));
+      }
+      if (need > 0) {
+        b->bscratch.alloc((size_t)need);
+        XCUDA(cudaMemsetAsync(b->bscratch.p, 0, b->bscratch.bytes(), s));
+      }
+      b->bstatus = w0.status.p;
       b->had_batched = true;
       b->had_T = (const float2*)fmms[0]->ops[0].m2l_T.p;
       b->had_nfreq = fmms[0]->nfreq;
@@ -3335,7 +3394,7 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
     XCUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     b->streams.push_back(st);
   }
-  while (b->events.size() < (size_t)3 * (nstreams + 1)) {
+  while (b->events.size() < (size_t)5 * (nstreams + 1)) {
     cudaEvent_t e;
     XCUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     b->events.push_back(e);
@@ -3359,33 +3418,55 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
       XCUDA(cudaStreamWaitEvent(s, b->events[evbase + 1 + j], 0));
     }
   };
-  // before the near field: upward pass, P2L, M2L and L2L per system; with one shared operator table the
-  // sparse M2L Hadamard of every system runs as one launch between the forward and backward transforms
-  const int pre1 = b->had_batched ? (M2L_FWD | M2L_HAD_DENSE) : M2L_ALL;
-  fork_join(0, [&](int k, cudaStream_t st) {
-    Fmm& f = *b->fmm[k];
-    Tree& t = *b->tree[k];
-    if (charges && charges[k]) set_charges(f, t, charges[k], true, st);
-    clear_values(f, t, st);
-    Workspace& ws = workspace(f, t, st);
-    dispatch(f, [&](auto e) {
-      decltype(e)::upward(f, t, ws, st);
-      decltype(e)::downward(f, t, ws, st, DOWN_PRE, pre1);
+  // before the near field: upward pass, P2L, M2L and L2L per system.  With one shared operator table (mixed
+  // Laplace) the parts that share it run as one launch over all systems: the M2M and L2L of each level, and
+  // the sparse M2L Hadamard between the systems' forward and backward transforms.
+  const int E = nstreams + 1;
+  Fmm& f0 = *b->fmm[0];
+  auto per_system = [&](int evbase, int up_parts, int pre_parts, bool first) {
+    fork_join(evbase, [&](int k, cudaStream_t st) {
+      Fmm& f = *b->fmm[k];
+      Tree& t = *b->tree[k];
+      if (first) {
+        if (charges && charges[k]) set_charges(f, t, charges[k], true, st);
+        clear_values(f, t, st);
+      }
+      Workspace& ws = workspace(f, t, st);
+      dispatch(f, [&](auto e) {
+        if (up_parts) decltype(e)::upward(f, t, ws, st, up_parts);
+        if (pre_parts) decltype(e)::downward(f, t, ws, st, DOWN_PRE, pre_parts);
+      });
     });
-  });
-  if (b->had_batched) {
+  };
+  auto batched_tr = [&](const GemmRows& g, bool m2m) {
+    if (g.M <= 0) return;
+    const int nn = f0.nsurf;
+    const LevelOps& op = f0.ops[0];
+    float* up0 = (float*)b->tree[0]->ws[f0.precision]->up.p;
+    float* dn0 = (float*)b->tree[0]->ws[f0.precision]->dn.p;
+    TGemm gg = m2m ? TGemm{g.M, nn, 8 * nn, g.a.p, g.c.p, nullptr, (int64_t)nn, 1, (int64_t)nn}
+                   : TGemm{g.M, 8 * nn, nn, g.a.p, g.c.p, nullptr, (int64_t)8 * nn, 1, (int64_t)nn};
+    gg.status = b->bstatus;
+    gg.scratch = b->bscratch.p;
+    gg.scratch_len = (int64_t)b->bscratch.n;
+    if (m2m) tgemm_tc<float>(gg, up0, op.tg_m2m_h.p, op.tg_m2m_l.p, op.ld_m2m, up0, s);
+    else tgemm_tc<float>(gg, dn0, op.tg_l2l_h.p, op.tg_l2l_l.p, op.ld_l2l, dn0, s);
+  };
+  if (!b->had_batched) {
+    per_system(0, UP_ALL, PRE_ALL, true);
+  } else {
+    per_system(0, UP_P2M, 0, true);
+    for (int l = (int)b->bm2m.size() - 1; l >= 0; l--) batched_tr(b->bm2m[l], true);
+    per_system(E, 0, M2L_FWD | M2L_HAD_DENSE, false);
     if (b->nhtiles > 0) {
       const int tpc = std::max(1, b->had_tpc);
       k_hadamard_rt_batch<<<dim3((b->nhtiles + tpc - 1) / tpc, b->had_nfreq), HADR_NT, HADT_SMEM, s>>>(
           b->had_T, b->hsys.p, b->htiles.p, b->nhtiles, tpc, b->had_nfreq);
       XLAUNCH();
     }
-    fork_join(2 * (nstreams + 1), [&](int k, cudaStream_t st) {
-      Fmm& f = *b->fmm[k];
-      Tree& t = *b->tree[k];
-      Workspace& ws = workspace(f, t, st);
-      dispatch(f, [&](auto e) { decltype(e)::downward(f, t, ws, st, DOWN_PRE, M2L_BWD); });
-    });
+    per_system(2 * E, 0, M2L_BWD, false);
+    for (int l = 0; l < (int)b->bl2l.size(); l++) batched_tr(b->bl2l[l], false);
+    per_system(3 * E, 0, PRE_DC2E, false);
   }
   // the near field of every system: one persistent launch draining the work queue
   if (b->nitems > 0) {
@@ -3415,7 +3496,7 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
       XLAUNCH();
     }
   }
-  fork_join(nstreams + 1, [&](int k, cudaStream_t st) {
+  fork_join(4 * E, [&](int k, cudaStream_t st) {
     Fmm& f = *b->fmm[k];
     Tree& t = *b->tree[k];
     Workspace& ws = workspace(f, t, st);
