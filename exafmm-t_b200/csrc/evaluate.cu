@@ -291,12 +291,9 @@ __device__ __forceinline__ void far_pair(double tx, double ty, double tz, const 
   gy = fma(-qi3, dy, gy);
   gz = fma(-qi3, dz, gz);
 }
+// the far field of evaluation leaf w (one warp); spw: the warp's FAR_CH staged surface points
 template <class W>
-__global__ void __launch_bounds__(32 * EVAL_WARPS) k_far_lap(EvalArgs a) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int w = blockIdx.x * EVAL_WARPS + wid;
-  if (w >= a.n_eval) return;
-  __shared__ double4 sp[EVAL_WARPS][FAR_CH];
+__device__ __forceinline__ void far_leaf_lap(const EvalArgs& a, int w, int lane, double4* spw) {
   const int pos = a.eval_leafs[w];
   const int node = a.leafs[pos];
   const int T = a.ntrgs[node];
@@ -326,9 +323,9 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_far_lap(EvalArgs a) {
         int j = sub;
         for (; j + 3 * G2 < cnt; j += 4 * G2) {
 #pragma unroll
-          for (int u = 0; u < 4; u++) far_pair(tx, ty, tz, sp[wid][j + u * G2], P[u], GX[u], GY[u], GZ[u]);
+          for (int u = 0; u < 4; u++) far_pair(tx, ty, tz, spw[j + u * G2], P[u], GX[u], GY[u], GZ[u]);
         }
-        for (; j < cnt; j += G2) far_pair(tx, ty, tz, sp[wid][j], P[0], GX[0], GY[0], GZ[0]);
+        for (; j < cnt; j += G2) far_pair(tx, ty, tz, spw[j], P[0], GX[0], GY[0], GZ[0]);
       }
       __syncwarp();
     };
@@ -341,7 +338,7 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_far_lap(EvalArgs a) {
         const int cnt = min(FAR_CH, n - j0);
         for (int i = lane; i < cnt; i += 32) {
           const int k = j0 + i;
-          sp[wid][i] = make_double4(cs.x + a.surf_base[3 * k] * b - c.x, cs.y + a.surf_base[3 * k + 1] * b - c.y,
+          spw[i] = make_double4(cs.x + a.surf_base[3 * k] * b - c.x, cs.y + a.surf_base[3 * k + 1] * b - c.y,
                                     cs.z + a.surf_base[3 * k + 2] * b - c.z, (double)upv[(int64_t)s * n + k]);
         }
         consume(cnt);
@@ -353,7 +350,7 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_far_lap(EvalArgs a) {
       const int cnt = min(FAR_CH, n - j0);
       for (int i = lane; i < cnt; i += 32) {
         const int k = j0 + i;
-        sp[wid][i] = make_double4(a.surf_base[3 * k] * b, a.surf_base[3 * k + 1] * b, a.surf_base[3 * k + 2] * b,
+        spw[i] = make_double4(a.surf_base[3 * k] * b, a.surf_base[3 * k + 1] * b, a.surf_base[3 * k + 2] * b,
                                   eqv[(int64_t)pos * n + k]);
       }
       consume(cnt);
@@ -373,6 +370,32 @@ __global__ void __launch_bounds__(32 * EVAL_WARPS) k_far_lap(EvalArgs a) {
       o[2] += gy * INV4PI;
       o[3] += gz * INV4PI;
     }
+  }
+}
+template <class W>
+__global__ void __launch_bounds__(32 * EVAL_WARPS) k_far_lap(EvalArgs a) {
+  __shared__ double4 sp[EVAL_WARPS][FAR_CH];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int w = blockIdx.x * EVAL_WARPS + wid;
+  if (w >= a.n_eval) return;
+  far_leaf_lap<W>(a, w, lane, sp[wid]);
+}
+// The far field of every system of a batch: each warp takes work items (system, evaluation leaf) from one
+// queue (a global counter, zeroed before the launch) in the order of `items` until it runs dry.
+template <class W>
+__global__ void __launch_bounds__(32 * EVAL_WARPS)
+    k_far_lap_queue(const EvalArgs* __restrict__ args, const int2* __restrict__ items, int64_t nitems,
+                    unsigned int* __restrict__ counter) {
+  __shared__ double4 sp[EVAL_WARPS][FAR_CH];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (;;) {
+    unsigned int k = 0;
+    if (lane == 0) k = atomicAdd(counter, 1u);
+    k = __shfl_sync(0xffffffffu, k, 0);
+    if ((int64_t)k >= nitems) break;
+    const int2 it = items[k];
+    far_leaf_lap<W>(args[it.x], it.y, lane, sp[wid]);
+    __syncwarp();
   }
 }
 
@@ -2939,6 +2962,17 @@ struct Engine {
     }
   }
 
+  // the far field (M2P + L2P evaluation), added to the near field's values
+  static EvalArgs far_args(Fmm& f, Tree& t, Workspace& ws) {
+    EvalArgs a{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.level.p, t.n_eval_leafs, t.sbeg.p,
+               t.tbeg.p,       t.center.p, t.src4.p,   t.trg4.p,  t.src_qim.p, t.p2p_off.p,  t.m2p_off.p,
+               t.p2p.p,        t.m2p.p,   f.surf_base.p, f.nsurf, ws.up.p,   ws.eq.p,        ws.out.p,
+               f.k_re,         f.k_im,    1,           1,         0,         1};
+    a.do_near = 0;
+    a.accumulate = 1;
+    return a;
+  }
+
   static NearArgs near_args(Fmm& f, Tree& t, Workspace& ws) {
     return NearArgs{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.n_eval_leafs, t.sbeg.p, t.tbeg.p,
                     t.p2p_off.p,    t.p2p.p,   t.center.p,  t.src4.p,  t.trg4.p,       t.src_qim.p, ws.out.p,
@@ -2970,13 +3004,8 @@ struct Engine {
     }
     if (phases & DOWN_NEAR) XCUDA(cudaEventRecord(ws.ev[8], s));
     if (t.n_eval_leafs && (phases & DOWN_FAR)) {
-      EvalArgs a{t.eval_leafs.p, t.leafs.p, t.nsrcs.p,   t.ntrgs.p, t.level.p,     t.n_eval_leafs, t.sbeg.p,
-                 t.tbeg.p,       t.center.p, t.src4.p,   t.trg4.p,  t.src_qim.p,   t.p2p_off.p,    t.m2p_off.p,
-                 t.p2p.p,        t.m2p.p,   f.surf_base.p, n,        ws.up.p,       ws.eq.p,        ws.out.p,
-                 f.k_re,         f.k_im,    1,           1,         0,             1};
+      const EvalArgs a = far_args(f, t, ws);
       const int blocks = nblk(t.n_eval_leafs, EVAL_WARPS);
-      a.do_near = 0;
-      a.accumulate = 1;
       if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
         k_far_lap<W><<<blocks, 32 * EVAL_WARPS, 0, s>>>(a);
       else
@@ -3206,6 +3235,11 @@ struct Batch {
   std::vector<GemmRows> bm2m, bl2l;  // row offsets rebased onto system 0's up / dn arrays
   DBuf<double> bscratch;             // FP64 scratch of their split K (zero between uses)
   int* bstatus = nullptr;            // system 0's device status flag (bounded waits)
+  // mixed Laplace: the far field of every system as one persistent launch over (system, leaf) items
+  DBuf<EvalArgs> fargs;
+  DBuf<int2> fitems;
+  int64_t nfitems = 0;
+  DBuf<unsigned int> fcounter;
   ~Batch() {
     for (auto e : events) cudaEventDestroy(e);
     for (auto st : streams) cudaStreamDestroy(st);
@@ -3245,6 +3279,30 @@ Batch* batch_create(Fmm** fmms, Tree** trees, int n, cudaStream_t s) {
       if (f.kernel == XFMM_LAPLACE && f.mixed() && ws.n_close < 0 && t.n_eval_leafs > 0)
         find_close_pairs(ws, hargs[k], t.n_eval_leafs, s);
       if (f.kernel == XFMM_LAPLACE && f.mixed()) b->nclose += std::max<int64_t>(ws.n_close, 0);
+    }
+    if (b->kernel == XFMM_LAPLACE && b->precision == XFMM_MIXED) {
+      // far-field items: evaluation leaves costed by targets x surface points evaluated (own + W list)
+      std::vector<EvalArgs> fa(n);
+      std::vector<std::pair<int64_t, int2>> fw;
+      for (int k = 0; k < n; k++) {
+        Fmm& f = *fmms[k];
+        Tree& t = *trees[k];
+        Workspace& ws = workspace(f, t, s);
+        fa[k] = Engine<K_LAPLACE, float>::far_args(f, t, ws);
+        std::vector<int64_t> moff = t.m2p_off.download(s);
+        std::vector<int> el = t.eval_leafs.download(s, (size_t)t.n_eval_leafs);
+        for (int i = 0; i < t.n_eval_leafs; i++) {
+          const int node = t.h_leafs[el[i]];
+          fw.push_back({(int64_t)t.h_ntrgs[node] * f.nsurf * (1 + moff[node + 1] - moff[node]), make_int2(k, i)});
+        }
+      }
+      std::stable_sort(fw.begin(), fw.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+      std::vector<int2> fi(fw.size());
+      for (size_t i = 0; i < fw.size(); i++) fi[i] = fw[i].second;
+      b->nfitems = (int64_t)fi.size();
+      if (!fi.empty()) b->fitems.upload(fi, s);
+      b->fargs.upload(fa, s);
+      b->fcounter.alloc(1);
     }
     std::stable_sort(work.begin(), work.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
     std::vector<int2> items(work.size());
@@ -3496,11 +3554,24 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
       XLAUNCH();
     }
   }
+  // the far field (one persistent launch over every system's leaves for mixed Laplace), then the results
+  const bool far_queue = b->nfitems > 0;
+  if (far_queue) {
+    int dev = 0, nsm = 148, per_sm = 0;
+    XCUDA(cudaGetDevice(&dev));
+    XCUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    XCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_far_lap_queue<float>, 32 * EVAL_WARPS, 0));
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * nsm, (b->nfitems + EVAL_WARPS - 1) / EVAL_WARPS));
+    XCUDA(cudaMemsetAsync(b->fcounter.p, 0, sizeof(unsigned int), s));
+    k_far_lap_queue<float><<<grid, 32 * EVAL_WARPS, 0, s>>>(b->fargs.p, b->fitems.p, b->nfitems, b->fcounter.p);
+    XLAUNCH();
+  }
   fork_join(4 * E, [&](int k, cudaStream_t st) {
     Fmm& f = *b->fmm[k];
     Tree& t = *b->tree[k];
     Workspace& ws = workspace(f, t, st);
-    dispatch(f, [&](auto e) { decltype(e)::downward(f, t, ws, st, DOWN_FAR); });
+    if (!far_queue) dispatch(f, [&](auto e) { decltype(e)::downward(f, t, ws, st, DOWN_FAR); });
     get_values(f, t, outs[k], st);
   });
 }
