@@ -351,9 +351,10 @@ def cpu_baseline(n, steps=3, warmup=1):
 
 def run_batched(args):
     """256 independent Laplace systems (N log-uniform in [2e3, 2e5], half cube, half Plummer), p=6,
-    ncrit=64, mixed precision: one CUDA-graph replay of the batched evaluate (per-system stages on
-    concurrent streams, one persistent near-field kernel over every system's target leaves) vs the
-    same evaluates launched one system at a time.  Aggregate particles/s over all systems."""
+    ncrit=64, mixed precision, one shared operator set: one CUDA-graph replay of the batched evaluate
+    (per-system stages on concurrent streams; M2M and L2L per level and the sparse M2L Hadamard as one
+    launch over all systems; persistent near-field and far-field kernels over every system's leaves) vs
+    the same evaluates launched one system at a time.  Aggregate particles/s over all systems."""
     import torch
     import exafmm.laplace as L
     from exafmm.batch import BatchedFmm, batched_workload
