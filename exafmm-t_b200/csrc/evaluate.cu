@@ -2706,40 +2706,40 @@ struct Engine {
   static void upward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int parts = UP_ALL) {
     const int n = f.nsurf;
     if (parts & UP_P2M) {
-    ws.launches = 0;
-    XCUDA(cudaEventRecord(ws.ev[0], s));
-    // P2M: check potentials of every leaf, then the pinv (UC2E) GEMM per leaf level
-    if (t.nleafs) {
-      SurfPotArgs a{t.leafs.p,  t.nleafs, t.nsrcs.p,     nullptr,  t.level.p, t.sbeg.p,   nullptr, t.center.p,
-                    t.src4.p,   t.src_qim.p, f.surf_base.p, n,      2.95,      ws.chk.p, 0,         f.k_re, f.k_im,
-                    INV4PI * op_scale(f, t)};
-      if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
-        k_surf_pot_lap_f2<<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
-      else
-        k_surf_pot<KER, R><<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
-      XLAUNCH();
-      ws.launches++;
-      // e = 0.5^l (V S+) (U^H c) per leaf level, two FP64 GEMMs on the tensor cores: y over the kept
-      // singular directions only, then e scattered to the leaves' up rows with the level's scale.
-      // (An FP32 first factor, as in L2P below, measured 1.4e-7 more potential error at p = 8 and 3e-7
-      // at p = 10: the upward densities feed every later translation.)
-      for (int l = 0; l <= t.depth; l++) {
-        if (KER == K_LAPLACE && l > 0) break;
-        const int r0 = ws.leaf_level_off[l], r1 = ws.leaf_level_off[l + 1];
-        const int m = KER == K_LAPLACE ? ws.p2m1.M : r1 - r0;
-        const int off = KER == K_LAPLACE ? 0 : r0;
-        if (m <= 0) continue;
-        const LevelOps& op = level_ops(f, l);
-        const int rk = op.rank;
-        TGemm g1{m, CW * rk, CW * n, ws.p2m1.a.p + off, ws.p2m1.c.p + off, nullptr, (int64_t)CW * n, 0, (int64_t)CW * n};
-        tgemm_f64<R, double>(g1, (const R*)ws.chk.p, op.tg_p2m1.p, (double*)ws.ybuf.p, s);
-        TGemm g2{m, CW * n, CW * rk, ws.p2m2.a.p + off, ws.p2m2.c.p + off, ws.p2m2.al64.p + off, (int64_t)CW * n, 0,
-                 (int64_t)CW * n};
-        tgemm_f64<double, R>(g2, (const double*)ws.ybuf.p, op.tg_p2m2.p, (R*)ws.up.p, s);
-        ws.launches += 2;
+      ws.launches = 0;
+      XCUDA(cudaEventRecord(ws.ev[0], s));
+      // P2M: check potentials of every leaf, then the pinv (UC2E) GEMM per leaf level
+      if (t.nleafs) {
+        SurfPotArgs a{t.leafs.p,  t.nleafs, t.nsrcs.p,     nullptr,  t.level.p, t.sbeg.p,   nullptr, t.center.p,
+                      t.src4.p,   t.src_qim.p, f.surf_base.p, n,      2.95,      ws.chk.p, 0,         f.k_re, f.k_im,
+                      INV4PI * op_scale(f, t)};
+        if constexpr (KER == K_LAPLACE && sizeof(R) == 4)
+          k_surf_pot_lap_f2<<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
+        else
+          k_surf_pot<KER, R><<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
+        XLAUNCH();
+        ws.launches++;
+        // e = 0.5^l (V S+) (U^H c) per leaf level, two FP64 GEMMs on the tensor cores: y over the kept
+        // singular directions only, then e scattered to the leaves' up rows with the level's scale.
+        // (An FP32 first factor, as in L2P below, measured 1.4e-7 more potential error at p = 8 and 3e-7
+        // at p = 10: the upward densities feed every later translation.)
+        for (int l = 0; l <= t.depth; l++) {
+          if (KER == K_LAPLACE && l > 0) break;
+          const int r0 = ws.leaf_level_off[l], r1 = ws.leaf_level_off[l + 1];
+          const int m = KER == K_LAPLACE ? ws.p2m1.M : r1 - r0;
+          const int off = KER == K_LAPLACE ? 0 : r0;
+          if (m <= 0) continue;
+          const LevelOps& op = level_ops(f, l);
+          const int rk = op.rank;
+          TGemm g1{m, CW * rk, CW * n, ws.p2m1.a.p + off, ws.p2m1.c.p + off, nullptr, (int64_t)CW * n, 0, (int64_t)CW * n};
+          tgemm_f64<R, double>(g1, (const R*)ws.chk.p, op.tg_p2m1.p, (double*)ws.ybuf.p, s);
+          TGemm g2{m, CW * n, CW * rk, ws.p2m2.a.p + off, ws.p2m2.c.p + off, ws.p2m2.al64.p + off, (int64_t)CW * n, 0,
+                   (int64_t)CW * n};
+          tgemm_f64<double, R>(g2, (const double*)ws.ybuf.p, op.tg_p2m2.p, (R*)ws.up.p, s);
+          ws.launches += 2;
+        }
       }
-    }
-    XCUDA(cudaEventRecord(ws.ev[1], s));
+      XCUDA(cudaEventRecord(ws.ev[1], s));
     }
     if (!(parts & UP_M2M)) return;
     // M2M: deepest parents first (post-order); per level one GEMM of the parents' 8 children rows
@@ -2776,169 +2776,169 @@ struct Engine {
       const int tab_level = KER == K_LAPLACE ? 0 : g + 1;
       const CT* T = (const CT*)f.ops[tab_level].m2l_T.p;
       if (phase & M2L_FWD) {
-      XCUDA(cudaEventRecord(ev[0], s));
-      // upward equivalent DFT (fmm_scale_invariant.h:560-604) -> specB [f][s][c]
-      if constexpr (KER != K_HELMHOLTZ) {
-        if (ws.fused) {
-          ft_dispatch(f.p, [&](auto pc) {
-            constexpr int PP = decltype(pc)::value;
-            const size_t smem = ftr_fwd_smem<R>(PP);
-            if (ws.ft_fwd_smem < smem) {
-              XCUDA(cudaFuncSetAttribute(k_m2l_fwd_r<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-              ws.ft_fwd_smem = smem;
-            }
-            k_m2l_fwd_r<R, PP><<<dim3(ns, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
-                src, ns, t.child0.p, (const R*)ws.up.p, n, f.conv_to_surf_up.p, f.dft_tw.p, (CT*)ws.specB.p);
-          });
-          XLAUNCH();
-          ws.launches++;
-        }
-      } else if (ws.fused) {
-        ftc_dispatch(f.p, [&](auto pc) {
-          constexpr int PP = decltype(pc)::value;
-          const size_t smem = ftc_fwd_smem<R>(PP);
-          if (ws.ft_fwd_smem < smem) {
-            XCUDA(cudaFuncSetAttribute(k_m2l_fwd_c<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            ws.ft_fwd_smem = smem;
-          }
-          k_m2l_fwd_c<R, PP><<<dim3(ns, 8 / FtcCpb<R>::v), FT_NT, smem, s>>>(
-              src, ns, t.child0.p, (const CT*)ws.up.p, n, f.conv_to_surf_up.p, f.dft_tw.p, (CT*)ws.specB.p);
-        });
-        XLAUNCH();
-        ws.launches++;
-      }
-      if (!ws.fused) {
-        k_m2l_grid_up<W><<<std::min<int64_t>(nblk((int64_t)ns * 8 * nconv), 148 * 32), 256, 0, s>>>(
-            src, ns, t.child0.p, (const W*)ws.up.p, n, f.conv_to_surf_up.p, nconv, (W*)ws.grid.p);
-        XLAUNCH();
-        ws.launches++;
-        XCUFFT2(cufftSetStream(ws.fwd[g], s));
-        exec_fwd(ws.fwd[g], ws.grid.p, ws.specA.p);
-        ws.launches++;
-        transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, (int64_t)ns * 8, nfreq, s);  // -> [f][s][c]
-      }
-      XCUDA(cudaEventRecord(ev[1], s));
-      }
-      if (phase & (M2L_HAD_SPARSE | M2L_HAD_DENSE)) {
-      // Hadamard product
-      const int ntiles = ws.had_tile0[g + 1] - ws.had_tile0[g];
-      if constexpr (sizeof(CT) == 8) {
-        XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
-        if (ntiles > 0 && (phase & M2L_HAD_SPARSE)) {
-          const int* rows = ws.hadr_row.p + (int64_t)ws.had_tile0[g] * HADR_TT;
-          if (!ws.hadrt_attr) {
-            XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
-            ws.hadrt_attr = true;
-          }
-          const int tpc = t.hadr_tpc > 0 ? t.hadr_tpc : HADR_TPC;
-          k_hadamard_rt<<<dim3((ntiles + tpc - 1) / tpc, nfreq), HADR_NT, HADT_SMEM, s>>>(
-              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
-              ws.hadr_ent.p, rows, ntiles, tpc, ns, nt, nfreq);
-          XLAUNCH();
-          ws.launches++;
-        }
-        if (ws.hadd_ld[g] > 0 && ws.had_tc5 && (phase & M2L_HAD_DENSE)) {
-          if (!ws.hadc_attr) {
-            XCUDA(cudaFuncSetAttribute(k_hadamard_dc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADC_SMEM));
-            ws.hadc_attr = true;
-          }
-          if (ws.hadc_btab_T != (const void*)T || ws.hadc_btab_nf != nfreq) {  // B blocks in the MMA layout
-            ws.hadc_btab.reserve((size_t)nfreq * HADC_BBYTES);
-            k_hadc_btab<<<std::min<int64_t>(nblk((int64_t)nfreq * 26 * 64), 148 * 16), 256, 0, s>>>(T, nfreq,
-                                                                                                  ws.hadc_btab.p);
+        XCUDA(cudaEventRecord(ev[0], s));
+        // upward equivalent DFT (fmm_scale_invariant.h:560-604) -> specB [f][s][c]
+        if constexpr (KER != K_HELMHOLTZ) {
+          if (ws.fused) {
+            ft_dispatch(f.p, [&](auto pc) {
+              constexpr int PP = decltype(pc)::value;
+              const size_t smem = ftr_fwd_smem<R>(PP);
+              if (ws.ft_fwd_smem < smem) {
+                XCUDA(cudaFuncSetAttribute(k_m2l_fwd_r<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                ws.ft_fwd_smem = smem;
+              }
+              k_m2l_fwd_r<R, PP><<<dim3(ns, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
+                  src, ns, t.child0.p, (const R*)ws.up.p, n, f.conv_to_surf_up.p, f.dft_tw.p, (CT*)ws.specB.p);
+            });
             XLAUNCH();
             ws.launches++;
-            ws.hadc_btab_T = T;
-            ws.hadc_btab_nf = nfreq;
           }
-          k_hadamard_dc<<<dim3(ws.hadd_ld[g] / 128, (nfreq + HADC_FPB - 1) / HADC_FPB), HADC_NT, HADC_SMEM, s>>>(
-              ws.hadc_btab.p, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
-              ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq, ws.status.p);
-          XLAUNCH();
-          ws.launches++;
-        } else if (ws.hadd_ld[g] > 0 && (phase & M2L_HAD_DENSE)) {
-          if (!ws.hadt_attr) {
-            XCUDA(cudaFuncSetAttribute(k_hadamard_dt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
-            ws.hadt_attr = true;
-          }
-          k_hadamard_dt<<<dim3((ws.hadd_ld[g] / HADT_TT + HADT_TPC - 1) / HADT_TPC, nfreq), HADT_NT, HADT_SMEM, s>>>(
-              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
-              ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
-          XLAUNCH();
-          ws.launches++;
-        }
-      } else {
-        XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
-        if (ws.hadd_ld[g] > 0 && (phase & M2L_HAD_DENSE)) {
-          if (!ws.had64_attr) {
-            XCUDA(cudaFuncSetAttribute(k_hadamard_d64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HAD64_SMEM));
-            ws.had64_attr = true;
-          }
-          k_hadamard_d64<<<dim3(ws.hadd_ld[g] / HAD64_TT, nfreq), HAD64_NT, HAD64_SMEM, s>>>(
-              T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
-              ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
-          XLAUNCH();
-          ws.launches++;
-        }
-      }
-      XCUDA(cudaEventRecord(ev[2], s));
-      }
-      if (phase & M2L_BWD) {
-      // inverse DFT of specA [f][t][c] to the downward check potentials (fmm_scale_invariant.h:606-646)
-      if constexpr (KER != K_HELMHOLTZ) {
-        if (ws.fused) {
-          ft_dispatch(f.p, [&](auto pc) {
+        } else if (ws.fused) {
+          ftc_dispatch(f.p, [&](auto pc) {
             constexpr int PP = decltype(pc)::value;
-          if constexpr (sizeof(R) == 4) {  // FP64: the unslabbed form (measured faster at 1 CTA per SM)
-            const size_t smem = ftr_bwd_smem<R>(PP);
-            if (ws.ft_bwd_smem < smem) {
-              XCUDA(cudaFuncSetAttribute(k_m2l_bwd_r<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-              ws.ft_bwd_smem = smem;
+            const size_t smem = ftc_fwd_smem<R>(PP);
+            if (ws.ft_fwd_smem < smem) {
+              XCUDA(cudaFuncSetAttribute(k_m2l_fwd_c<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+              ws.ft_fwd_smem = smem;
             }
-            k_m2l_bwd_r<R, PP><<<dim3(nt, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
-                trg, nt, t.child0.p, (const CT*)ws.specA.p, n, f.map_dn.p, f.dft_tw.p,
-                m2l_scale_of<R>(t) + t.m2l_trg_off[g], (R*)ws.dn.p);
-          } else {
-            const size_t smem = ft_bwd_smem<R>(PP);
-            if (ws.ft_bwd_smem < smem) {
-              XCUDA(cudaFuncSetAttribute(k_m2l_bwd<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-              ws.ft_bwd_smem = smem;
-            }
-            k_m2l_bwd<R, PP><<<dim3(nt, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
-                trg, nt, t.child0.p, (const CT*)ws.specA.p, n, f.map_dn.p, f.dft_tw.p,
-                m2l_scale_of<R>(t) + t.m2l_trg_off[g], (R*)ws.dn.p);
-          }
+            k_m2l_fwd_c<R, PP><<<dim3(ns, 8 / FtcCpb<R>::v), FT_NT, smem, s>>>(
+                src, ns, t.child0.p, (const CT*)ws.up.p, n, f.conv_to_surf_up.p, f.dft_tw.p, (CT*)ws.specB.p);
           });
           XLAUNCH();
           ws.launches++;
         }
-      } else if (ws.fused) {
-        ftc_dispatch(f.p, [&](auto pc) {
-          constexpr int PP = decltype(pc)::value;
-          const size_t smem = ftc_bwd_smem<R>(PP);
-          if (ws.ft_bwd_smem < smem) {
-            XCUDA(cudaFuncSetAttribute(k_m2l_bwd_c<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            ws.ft_bwd_smem = smem;
+        if (!ws.fused) {
+          k_m2l_grid_up<W><<<std::min<int64_t>(nblk((int64_t)ns * 8 * nconv), 148 * 32), 256, 0, s>>>(
+              src, ns, t.child0.p, (const W*)ws.up.p, n, f.conv_to_surf_up.p, nconv, (W*)ws.grid.p);
+          XLAUNCH();
+          ws.launches++;
+          XCUFFT2(cufftSetStream(ws.fwd[g], s));
+          exec_fwd(ws.fwd[g], ws.grid.p, ws.specA.p);
+          ws.launches++;
+          transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, (int64_t)ns * 8, nfreq, s);  // -> [f][s][c]
+        }
+        XCUDA(cudaEventRecord(ev[1], s));
+      }
+      if (phase & (M2L_HAD_SPARSE | M2L_HAD_DENSE)) {
+        // Hadamard product
+        const int ntiles = ws.had_tile0[g + 1] - ws.had_tile0[g];
+        if constexpr (sizeof(CT) == 8) {
+          XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
+          if (ntiles > 0 && (phase & M2L_HAD_SPARSE)) {
+            const int* rows = ws.hadr_row.p + (int64_t)ws.had_tile0[g] * HADR_TT;
+            if (!ws.hadrt_attr) {
+              XCUDA(cudaFuncSetAttribute(k_hadamard_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
+              ws.hadrt_attr = true;
+            }
+            const int tpc = t.hadr_tpc > 0 ? t.hadr_tpc : HADR_TPC;
+            k_hadamard_rt<<<dim3((ntiles + tpc - 1) / tpc, nfreq), HADR_NT, HADT_SMEM, s>>>(
+                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadr_tile.p + ws.had_tile0[g], ws.hadr_pos.p,
+                ws.hadr_ent.p, rows, ntiles, tpc, ns, nt, nfreq);
+            XLAUNCH();
+            ws.launches++;
           }
-          k_m2l_bwd_c<R, PP><<<dim3(nt, 8 / FtcCpb<R>::v), FT_NT, smem, s>>>(trg, nt, t.child0.p, (const CT*)ws.specA.p, n,
-                                                             f.map_dn.p, f.dft_tw.p,
-                                                             m2l_scale_of<R>(t) + t.m2l_trg_off[g], (CT*)ws.dn.p);
-        });
-        XLAUNCH();
-        ws.launches++;
+          if (ws.hadd_ld[g] > 0 && ws.had_tc5 && (phase & M2L_HAD_DENSE)) {
+            if (!ws.hadc_attr) {
+              XCUDA(cudaFuncSetAttribute(k_hadamard_dc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADC_SMEM));
+              ws.hadc_attr = true;
+            }
+            if (ws.hadc_btab_T != (const void*)T || ws.hadc_btab_nf != nfreq) {  // B blocks in the MMA layout
+              ws.hadc_btab.reserve((size_t)nfreq * HADC_BBYTES);
+              k_hadc_btab<<<std::min<int64_t>(nblk((int64_t)nfreq * 26 * 64), 148 * 16), 256, 0, s>>>(T, nfreq,
+                                                                                                    ws.hadc_btab.p);
+              XLAUNCH();
+              ws.launches++;
+              ws.hadc_btab_T = T;
+              ws.hadc_btab_nf = nfreq;
+            }
+            k_hadamard_dc<<<dim3(ws.hadd_ld[g] / 128, (nfreq + HADC_FPB - 1) / HADC_FPB), HADC_NT, HADC_SMEM, s>>>(
+                ws.hadc_btab.p, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+                ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq, ws.status.p);
+            XLAUNCH();
+            ws.launches++;
+          } else if (ws.hadd_ld[g] > 0 && (phase & M2L_HAD_DENSE)) {
+            if (!ws.hadt_attr) {
+              XCUDA(cudaFuncSetAttribute(k_hadamard_dt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HADT_SMEM));
+              ws.hadt_attr = true;
+            }
+            k_hadamard_dt<<<dim3((ws.hadd_ld[g] / HADT_TT + HADT_TPC - 1) / HADT_TPC, nfreq), HADT_NT, HADT_SMEM, s>>>(
+                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+                ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
+            XLAUNCH();
+            ws.launches++;
+          }
+        } else {
+          XREQUIRE(nfreq < 65536, XFMM_ERR_UNSUPPORTED, "too many frequencies for the Hadamard grid");
+          if (ws.hadd_ld[g] > 0 && (phase & M2L_HAD_DENSE)) {
+            if (!ws.had64_attr) {
+              XCUDA(cudaFuncSetAttribute(k_hadamard_d64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HAD64_SMEM));
+              ws.had64_attr = true;
+            }
+            k_hadamard_d64<<<dim3(ws.hadd_ld[g] / HAD64_TT, nfreq), HAD64_NT, HAD64_SMEM, s>>>(
+                T, (const CT*)ws.specB.p, (CT*)ws.specA.p, ws.hadd_tab.p + ws.hadd_tab0[g], ws.hadd_ld[g],
+                ws.hadd_row.p + ws.hadd_row0[g], ns, nt, nfreq);
+            XLAUNCH();
+            ws.launches++;
+          }
+        }
+        XCUDA(cudaEventRecord(ev[2], s));
       }
-      if (!ws.fused) {
-        ws.launches++;
-        transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, nfreq, (int64_t)nt * 8, s);  // -> [t][c][f]
-        XCUFFT2(cufftSetStream(ws.bwd[g], s));
-        exec_bwd(ws.bwd[g], ws.specB.p, ws.grid.p);
-        k_m2l_gather_dn<W, R><<<std::min<int64_t>(nblk((int64_t)nt * 8 * n), 148 * 32), 256, 0, s>>>(
-            trg, nt, t.child0.p, (const W*)ws.grid.p, nconv, f.map_dn.p, n,
-            m2l_scale_of<R>(t) + t.m2l_trg_off[g], (W*)ws.dn.p);
-        XLAUNCH();
-        ws.launches += 2;
-      }
-      XCUDA(cudaEventRecord(ev[3], s));
+      if (phase & M2L_BWD) {
+        // inverse DFT of specA [f][t][c] to the downward check potentials (fmm_scale_invariant.h:606-646)
+        if constexpr (KER != K_HELMHOLTZ) {
+          if (ws.fused) {
+            ft_dispatch(f.p, [&](auto pc) {
+              constexpr int PP = decltype(pc)::value;
+            if constexpr (sizeof(R) == 4) {  // FP64: the unslabbed form (measured faster at 1 CTA per SM)
+              const size_t smem = ftr_bwd_smem<R>(PP);
+              if (ws.ft_bwd_smem < smem) {
+                XCUDA(cudaFuncSetAttribute(k_m2l_bwd_r<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                ws.ft_bwd_smem = smem;
+              }
+              k_m2l_bwd_r<R, PP><<<dim3(nt, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
+                  trg, nt, t.child0.p, (const CT*)ws.specA.p, n, f.map_dn.p, f.dft_tw.p,
+                  m2l_scale_of<R>(t) + t.m2l_trg_off[g], (R*)ws.dn.p);
+            } else {
+              const size_t smem = ft_bwd_smem<R>(PP);
+              if (ws.ft_bwd_smem < smem) {
+                XCUDA(cudaFuncSetAttribute(k_m2l_bwd<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                ws.ft_bwd_smem = smem;
+              }
+              k_m2l_bwd<R, PP><<<dim3(nt, 8 / FtCpb<R>::v), FT_NT, smem, s>>>(
+                  trg, nt, t.child0.p, (const CT*)ws.specA.p, n, f.map_dn.p, f.dft_tw.p,
+                  m2l_scale_of<R>(t) + t.m2l_trg_off[g], (R*)ws.dn.p);
+            }
+            });
+            XLAUNCH();
+            ws.launches++;
+          }
+        } else if (ws.fused) {
+          ftc_dispatch(f.p, [&](auto pc) {
+            constexpr int PP = decltype(pc)::value;
+            const size_t smem = ftc_bwd_smem<R>(PP);
+            if (ws.ft_bwd_smem < smem) {
+              XCUDA(cudaFuncSetAttribute(k_m2l_bwd_c<R, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+              ws.ft_bwd_smem = smem;
+            }
+            k_m2l_bwd_c<R, PP><<<dim3(nt, 8 / FtcCpb<R>::v), FT_NT, smem, s>>>(trg, nt, t.child0.p, (const CT*)ws.specA.p, n,
+                                                               f.map_dn.p, f.dft_tw.p,
+                                                               m2l_scale_of<R>(t) + t.m2l_trg_off[g], (CT*)ws.dn.p);
+          });
+          XLAUNCH();
+          ws.launches++;
+        }
+        if (!ws.fused) {
+          ws.launches++;
+          transpose<CT>((const CT*)ws.specA.p, (CT*)ws.specB.p, nfreq, (int64_t)nt * 8, s);  // -> [t][c][f]
+          XCUFFT2(cufftSetStream(ws.bwd[g], s));
+          exec_bwd(ws.bwd[g], ws.specB.p, ws.grid.p);
+          k_m2l_gather_dn<W, R><<<std::min<int64_t>(nblk((int64_t)nt * 8 * n), 148 * 32), 256, 0, s>>>(
+              trg, nt, t.child0.p, (const W*)ws.grid.p, nconv, f.map_dn.p, n,
+              m2l_scale_of<R>(t) + t.m2l_trg_off[g], (W*)ws.dn.p);
+          XLAUNCH();
+          ws.launches += 2;
+        }
+        XCUDA(cudaEventRecord(ev[3], s));
       }
     }
   }
@@ -3034,23 +3034,23 @@ struct Engine {
     if (t.n_m2l_trg) m2l(f, t, ws, s, m2l_phase);
     if (m2l_phase & M2L_BWD) XCUDA(cudaEventRecord(ws.ev[4], s));
     if (m2l_phase & PRE_L2L) {
-    // L2L: shallowest parents first (pre-order); per level one GEMM of the parents' rows with the
-    // [n][8n] operator, added to the 8 children rows (contiguous per parent)
-    for (int l = 0; l < t.depth; l++) {
-      const GemmRows& g = ws.l2l[l];
-      if (g.M <= 0) continue;
-      const LevelOps& op = level_ops(f, l);
-      TGemm gl{g.M, CW * 8 * n, CW * n, g.a.p, g.c.p, nullptr, (int64_t)CW * 8 * n, 1, (int64_t)CW * n};
-      gl.status = ws.status.p;
-      gl.scratch = ws.tc_scratch.p;
-      gl.scratch_len = (int64_t)ws.tc_scratch.n;
-      if constexpr (sizeof(R) == 4)
-        tgemm_tc<float>(gl, (const float*)ws.dn.p, op.tg_l2l_h.p, op.tg_l2l_l.p, op.ld_l2l, (float*)ws.dn.p, s);
-      else
-        tgemm_f64<double, double>(gl, (const double*)ws.dn.p, op.tg_l2l.p, (double*)ws.dn.p, s);
-      ws.launches++;
-    }
-    XCUDA(cudaEventRecord(ws.ev[5], s));
+      // L2L: shallowest parents first (pre-order); per level one GEMM of the parents' rows with the
+      // [n][8n] operator, added to the 8 children rows (contiguous per parent)
+      for (int l = 0; l < t.depth; l++) {
+        const GemmRows& g = ws.l2l[l];
+        if (g.M <= 0) continue;
+        const LevelOps& op = level_ops(f, l);
+        TGemm gl{g.M, CW * 8 * n, CW * n, g.a.p, g.c.p, nullptr, (int64_t)CW * 8 * n, 1, (int64_t)CW * n};
+        gl.status = ws.status.p;
+        gl.scratch = ws.tc_scratch.p;
+        gl.scratch_len = (int64_t)ws.tc_scratch.n;
+        if constexpr (sizeof(R) == 4)
+          tgemm_tc<float>(gl, (const float*)ws.dn.p, op.tg_l2l_h.p, op.tg_l2l_l.p, op.ld_l2l, (float*)ws.dn.p, s);
+        else
+          tgemm_f64<double, double>(gl, (const double*)ws.dn.p, op.tg_l2l.p, (double*)ws.dn.p, s);
+        ws.launches++;
+      }
+      XCUDA(cudaEventRecord(ws.ev[5], s));
     }
     if (!(m2l_phase & PRE_DC2E)) return;
     // L2P part 1: downward check -> equivalent (DC2E) per leaf level, e = conj(U) S+ (conj(VH) 0.5^l c):
