@@ -2692,8 +2692,8 @@ constexpr int M2L_FWD = 1, M2L_HAD_SPARSE = 2, M2L_HAD_DENSE = 4, M2L_BWD = 8, M
 // parts of the downward pass before the near field: the M2L parts above (P2L with the forward transforms),
 // then L2L, then L2P's check-to-equivalent step
 constexpr int PRE_L2L = 16, PRE_DC2E = 32, PRE_ALL = M2L_ALL | PRE_L2L | PRE_DC2E;
-// parts of the upward pass
-constexpr int UP_P2M = 1, UP_M2M = 2, UP_ALL = 3;
+// parts of the upward pass: P2M's check potentials, its two pseudo-inverse GEMMs, M2M
+constexpr int UP_CHK = 1, UP_M2M = 2, UP_PINV = 4, UP_P2M = UP_CHK | UP_PINV, UP_ALL = 7;
 
 // ------------------------------------------------------------------ engine, per kernel and precision
 template <int KER, class R>
@@ -2706,10 +2706,12 @@ struct Engine {
   static void upward(Fmm& f, Tree& t, Workspace& ws, cudaStream_t s, int parts = UP_ALL) {
     const int n = f.nsurf;
     if (parts & UP_P2M) {
-      ws.launches = 0;
-      XCUDA(cudaEventRecord(ws.ev[0], s));
+      if (parts & UP_CHK) {
+        ws.launches = 0;
+        XCUDA(cudaEventRecord(ws.ev[0], s));
+      }
       // P2M: check potentials of every leaf, then the pinv (UC2E) GEMM per leaf level
-      if (t.nleafs) {
+      if (t.nleafs && (parts & UP_CHK)) {
         SurfPotArgs a{t.leafs.p,  t.nleafs, t.nsrcs.p,     nullptr,  t.level.p, t.sbeg.p,   nullptr, t.center.p,
                       t.src4.p,   t.src_qim.p, f.surf_base.p, n,      2.95,      ws.chk.p, 0,         f.k_re, f.k_im,
                       INV4PI * op_scale(f, t)};
@@ -2719,6 +2721,8 @@ struct Engine {
           k_surf_pot<KER, R><<<nblk(t.nleafs, 4), 128, 0, s>>>(a);
         XLAUNCH();
         ws.launches++;
+      }
+      if (t.nleafs && (parts & UP_PINV)) {
         // e = 0.5^l (V S+) (U^H c) per leaf level, two FP64 GEMMs on the tensor cores: y over the kept
         // singular directions only, then e scattered to the leaves' up rows with the level's scale.
         // (An FP32 first factor, as in L2P below, measured 1.4e-7 more potential error at p = 8 and 3e-7
@@ -2739,7 +2743,7 @@ struct Engine {
           ws.launches += 2;
         }
       }
-      XCUDA(cudaEventRecord(ws.ev[1], s));
+      if (parts & UP_PINV) XCUDA(cudaEventRecord(ws.ev[1], s));
     }
     if (!(parts & UP_M2M)) return;
     // M2M: deepest parents first (post-order); per level one GEMM of the parents' 8 children rows
@@ -3234,6 +3238,7 @@ struct Batch {
   // with the shared table also the M2M and L2L of every system, per level one GEMM over all systems' rows
   std::vector<GemmRows> bm2m, bl2l;  // row offsets rebased onto system 0's up / dn arrays
   DBuf<double> bscratch;             // FP64 scratch of their split K (zero between uses)
+  GemmRows bp2m1, bp2m2, bl2p1, bl2p2;  // P2M and L2P pseudo-inverse factors of every system's leaves
   int* bstatus = nullptr;            // system 0's device status flag (bounded waits)
   // mixed Laplace: the far field of every system as one persistent launch over (system, leaf) items
   DBuf<EvalArgs> fargs;
@@ -3385,6 +3390,45 @@ Batch* batch_create(Fmm** fmms, Tree** trees, int n, cudaStream_t s) {
         need = std::max(need, tgemm_tc_scratch((int)ma.size(), ns, 8 * ns, 1));
         need = std::max(need, tgemm_tc_scratch((int)la.size(), 8 * ns, ns, 1));
       }
+      // the pseudo-inverse factors of P2M and L2P over every system's leaves (one leaf group for Laplace):
+      // A and C offsets rebased onto system 0's arrays, each in its own element unit
+      {
+        auto rel = [](const DBuf<char>& x, const DBuf<char>& x0, size_t es) {
+          return (int64_t)((x.p - x0.p) / (int64_t)es);
+        };
+        std::vector<int64_t> a1, c1, a2, c2, la1, lc1, la2, lc2;
+        std::vector<double> al2, lal1;
+        for (int k = 0; k < n; k++) {
+          Workspace& ws = *trees[k]->ws[prec];
+          const int64_t dchk = rel(ws.chk, w0.chk, sizeof(float)), dy = rel(ws.ybuf, w0.ybuf, sizeof(double)),
+                        dup = rel(ws.up, w0.up, sizeof(float)), ddn = rel(ws.dn, w0.dn, sizeof(float)),
+                        deq = rel(ws.eq, w0.eq, sizeof(double));
+          auto take = [&](const GemmRows& g, int64_t da, int64_t dc, std::vector<int64_t>& va,
+                          std::vector<int64_t>& vc, std::vector<double>* val) {
+            if (g.M <= 0) return;
+            const std::vector<int64_t> a = g.a.download(s, (size_t)g.M), c = g.c.download(s, (size_t)g.M);
+            std::vector<double> al;
+            if (val) al = g.al64.download(s, (size_t)g.M);
+            for (int i = 0; i < g.M; i++) {
+              va.push_back(a[i] + da);
+              vc.push_back(c[i] + dc);
+              if (val) val->push_back(al[i]);
+            }
+          };
+          XREQUIRE(ws.p2m1.M == ws.p2m2.M && ws.l2p1.M == ws.l2p2.M, XFMM_ERR_STATE,
+                   "pseudo-inverse factor rows differ");
+          take(ws.p2m1, dchk, dy, a1, c1, nullptr);
+          take(ws.p2m2, dy, dup, a2, c2, &al2);
+          take(ws.l2p1, ddn, dy, la1, lc1, nullptr);
+          // L2P's first factor takes its per-row scale from the second factor's rows (as in the evaluate)
+          take(ws.l2p2, dy, deq, la2, lc2, &lal1);
+        }
+        upload_rows<double>(b->bp2m1, a1, c1, std::vector<double>(a1.size(), 1.0), s);
+        upload_rows<double>(b->bp2m2, a2, c2, al2, s);
+        upload_rows<double>(b->bl2p1, la1, lc1, lal1, s);
+        upload_rows<double>(b->bl2p2, la2, lc2, std::vector<double>(la2.size(), 1.0), s);
+        need = std::max(need, tgemm_tc_scratch((int)la1.size(), fmms[0]->ops[0].rank, ns, 0));
+      }
       if (need > 0) {
         b->bscratch.alloc((size_t)need);
         XCUDA(cudaMemsetAsync(b->bscratch.p, 0, b->bscratch.bytes(), s));
@@ -3513,7 +3557,16 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
   if (!b->had_batched) {
     per_system(0, UP_ALL, PRE_ALL, true);
   } else {
-    per_system(0, UP_P2M, 0, true);
+    Workspace& w0 = *b->tree[0]->ws[f0.precision];
+    const int nn = f0.nsurf, rk = f0.ops[0].rank;
+    const LevelOps& op = f0.ops[0];
+    per_system(0, UP_CHK, 0, true);
+    if (b->bp2m1.M > 0) {  // P2M's pseudo-inverse factors of every system's leaves
+      TGemm g1{b->bp2m1.M, rk, nn, b->bp2m1.a.p, b->bp2m1.c.p, nullptr, (int64_t)nn, 0, (int64_t)nn};
+      tgemm_f64<float, double>(g1, (const float*)w0.chk.p, op.tg_p2m1.p, (double*)w0.ybuf.p, s);
+      TGemm g2{b->bp2m2.M, nn, rk, b->bp2m2.a.p, b->bp2m2.c.p, b->bp2m2.al64.p, (int64_t)nn, 0, (int64_t)nn};
+      tgemm_f64<double, float>(g2, (const double*)w0.ybuf.p, op.tg_p2m2.p, (float*)w0.up.p, s);
+    }
     for (int l = (int)b->bm2m.size() - 1; l >= 0; l--) batched_tr(b->bm2m[l], true);
     per_system(E, 0, M2L_FWD | M2L_HAD_DENSE, false);
     if (b->nhtiles > 0) {
@@ -3524,7 +3577,15 @@ void batch_evaluate(Batch* b, const double* const* charges, double* const* outs,
     }
     per_system(2 * E, 0, M2L_BWD, false);
     for (int l = 0; l < (int)b->bl2l.size(); l++) batched_tr(b->bl2l[l], false);
-    per_system(3 * E, 0, PRE_DC2E, false);
+    if (b->bl2p1.M > 0) {  // L2P's check-to-equivalent factors of every system's leaves
+      TGemm g1{b->bl2p1.M, rk, nn, b->bl2p1.a.p, b->bl2p1.c.p, b->bl2p1.al64.p, (int64_t)nn, 0, (int64_t)nn};
+      g1.status = b->bstatus;
+      g1.scratch = b->bscratch.p;
+      g1.scratch_len = (int64_t)b->bscratch.n;
+      tgemm_tc<double>(g1, (const float*)w0.dn.p, op.tg_l2p1_h.p, op.tg_l2p1_l.p, op.ld_l2p1, (double*)w0.ybuf.p, s);
+      TGemm g2{b->bl2p2.M, nn, rk, b->bl2p2.a.p, b->bl2p2.c.p, nullptr, (int64_t)nn, 0, (int64_t)nn};
+      tgemm_f64<double, double>(g2, (const double*)w0.ybuf.p, op.tg_l2p2.p, (double*)w0.eq.p, s);
+    }
   }
   // the near field of every system: one persistent launch draining the work queue
   if (b->nitems > 0) {
