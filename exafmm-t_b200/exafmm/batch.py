@@ -6,8 +6,8 @@ share one Fmm object: its scale-invariant operators, precomputed once for the fi
 serve every other radius (the evaluate scales the body-to-check potentials by the ratio of the radii);
 the other kernels' operators depend on the radius, so each of those systems gets its own Fmm object.
 With one shared operator table (mixed Laplace) the work that shares it is one launch over all systems:
-the M2M and L2L of each level, and the sparse M2L Hadamard between the systems' forward and backward M2L
-transforms.  The systems are held by one native batch (xfmm_batch_*):
+the pseudo-inverse factors of P2M and L2P, the M2M and L2L of each level, the sparse M2L Hadamard between
+the systems' forward and backward M2L transforms, and the far field.  The systems are held by one native batch (xfmm_batch_*):
 one evaluate of every system runs each system's stages before and after its near field on concurrent
 streams forked from the batch stream (largest systems first, each to the least-loaded stream), and the
 near field of all systems as one persistent kernel that drains a work queue of (system, target leaf)

@@ -148,8 +148,9 @@ xfmm_status xfmm_set_tuning(xfmm_tree* tree, int option, int value);
  * systems is one persistent kernel draining a work queue of (system, target leaf) items, largest first,
  * and the exact close-pair corrections of all systems one more launch.  When every system uses the same
  * xfmm_fmm handle, mixed Laplace with one scale-invariant operator set, the work that shares the operators
- * is one launch over all systems too: the M2M and the L2L of each level, and the sparse M2L Hadamard
- * between the systems' forward and backward M2L transforms.  Asynchronous on `stream`, no
+ * is one launch over all systems too: the pseudo-inverse factors of P2M and L2P, the M2M and the L2L of
+ * each level, the sparse M2L Hadamard between the systems' forward and backward M2L transforms, and the
+ * far field (a persistent kernel over (system, leaf) items).  Asynchronous on `stream`, no
  * allocation: it may be captured into a CUDA graph (after one evaluate outside the capture). */
 typedef struct xfmm_batch xfmm_batch;
 enum {
