@@ -12,16 +12,17 @@
 // A complex translation is a real one of twice the size: interleaved complex rows are real rows, and
 // the operator is expanded to [2K][2N] with the 2x2 blocks (re, im; -im, re) (expand_operator).
 //
-// Two kernels, both 64 x 64 output tiles per CTA of 4 warps (2 x 2 warps of 32 x 32), K in steps of 16
-// staged through shared memory (k-major, padded rows), next step prefetched into registers:
-//   k_tgemm_f64   FP64 on the FP64 tensor path (mma.sync m8n8k4 f64): pseudo-inverse factors (their
+// Two kernels:
+//   k_tgemm_f64   FP64 on the FP64 tensor path (mma.sync m8n8k4 f64), 64 x 64 output tiles per CTA of 4
+//                 warps, K in steps of 16 staged through shared memory: pseudo-inverse factors (their
 //                 1/s amplification needs FP64) and every translation of the FP64 path.
-//   k_tgemm_tf32  FP32 accuracy from three TF32 tensor-core products of head/tail splits
-//                 (Ah Bh + Ah Bt + At Bh, the tail-tail term 2^-22 relative dropped) for the mixed path's
-//                 M2M, L2L and L2P's first factor.  B is split once per operator (hi/lo arrays).  Each
-//                 16-wide K step is formed in a fresh MMA accumulator and added to FP32 running sums
-//                 with round-to-nearest adds: the tensor core's own FP32 accumulation truncates, and over
-//                 the 2368-term M2M rows it would cost accuracy.
+//   k_tgemm_tc    FP32 accuracy from three TF32 tensor-core products of head/tail splits
+//                 (Ah Bh + Ah Bt + At Bh, the tail-tail term 2^-22 relative dropped) on tcgen05 with
+//                 TMEM accumulators, for the mixed path's M2M, L2L and L2P's first factor.  B is split
+//                 once per operator (hi/lo arrays).  Each 16-wide K step is formed in a fresh MMA
+//                 accumulator and added to FP32 running sums with round-to-nearest adds: the tensor
+//                 core's own FP32 accumulation truncates, and over the 2368-term M2M rows it would cost
+//                 accuracy.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -174,143 +175,8 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& h, uint32_t& l) {
   h = tf32_round(x);
   l = tf32_round(x - __uint_as_float(h));
 }
-__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// C[coff[r] + j] (=|+=) alpha[r] * sum_k A[aoff[r] + k] * (Bh + Bl)[k * ldb + j] with FP32 A.
-// A row-major in shared memory ([BM][BK + 4]), Bh and Bl k-major ([BK][BN + 8]), cp.async ring of TGT_ST
-// stages.  Warp (wm, wn) owns rows 32 wm .. +31 (2 m16 fragments) and columns 32 wn .. +31 (4 n8
-// fragments); lane (g, t) holds A[g | g+8][t | t+4], B[t | t+4][g] and C[g | g+8][2t .. 2t + 1].
-constexpr int TGT_BK = 16, TGT_ST = 3, TGT_LDA = TGT_BK + 4, TGT_LDB = TG_BN + 8;  // 43 KB: 4 CTAs per SM
-constexpr size_t TGT_SMEM = (size_t)TGT_ST * ((size_t)TG_BM * TGT_LDA + 2 * (size_t)TGT_BK * TGT_LDB) * sizeof(float);
-
-template <class TC, int VB>
-__global__ void __launch_bounds__(TG_NT, 4) k_tgemm_tf32(int M, int N, int K, const float* __restrict__ A,
-                                                       const int64_t* __restrict__ aoff, const float* __restrict__ Bh,
-                                                       const float* __restrict__ Bl, int64_t ldb,
-                                                       const double* __restrict__ alpha, TC* __restrict__ C,
-                                                       const int64_t* __restrict__ coff, int acc) {
-  extern __shared__ __align__(16) float tgt_sm[];
-  float* As = tgt_sm;
-  float* Hs = As + (size_t)TGT_ST * TG_BM * TGT_LDA;
-  float* Ls = Hs + (size_t)TGT_ST * TGT_BK * TGT_LDB;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wm = w >> 1, wn = w & 1;
-  const int g = lane >> 2, t = lane & 3;
-  const int m0 = blockIdx.x * TG_BM, n0 = blockIdx.y * TG_BN;
-  const int nk = (K + TGT_BK - 1) / TGT_BK;
-  auto load = [&](int slot, int kt) {
-    const int k0 = kt * TGT_BK;
-    tile_async<VB, 4>(
-        reinterpret_cast<char*>(As + (size_t)slot * TG_BM * TGT_LDA), TG_BM, TGT_BK, TGT_LDA,
-        [&](int i) -> const char* {
-          const int r = m0 + i;
-          return r < M ? reinterpret_cast<const char*>(A + aoff[r]) : nullptr;
-        },
-        k0, K, A);
-    auto brow = [&](const float* Bx) {
-      return [=](int i) -> const char* {
-        const int k = k0 + i;
-        return k < K ? reinterpret_cast<const char*>(Bx + (int64_t)k * ldb) : nullptr;
-      };
-    };
-    tile_async<VB, 4>(reinterpret_cast<char*>(Hs + (size_t)slot * TGT_BK * TGT_LDB), TGT_BK, TG_BN, TGT_LDB, brow(Bh),
-                      n0, N, Bh);
-    tile_async<VB, 4>(reinterpret_cast<char*>(Ls + (size_t)slot * TGT_BK * TGT_LDB), TGT_BK, TG_BN, TGT_LDB, brow(Bl),
-                      n0, N, Bl);
-  };
-  float run[2][4][4];  // round-to-nearest running sums
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int e = 0; e < 4; e++) run[i][j][e] = 0.f;
-#pragma unroll
-  for (int st = 0; st < TGT_ST - 1; st++) {
-    if (st < nk) load(st, st);
-    cp_commit();
-  }
-  for (int kt = 0; kt < nk; kt++) {
-    cp_wait<TGT_ST - 2>();
-    __syncthreads();
-    const int nx = kt + TGT_ST - 1;
-    if (nx < nk) load(nx % TGT_ST, nx);
-    cp_commit();
-    const float* a_s = As + (size_t)(kt % TGT_ST) * TG_BM * TGT_LDA;
-    const float* h_s = Hs + (size_t)(kt % TGT_ST) * TGT_BK * TGT_LDB;
-    const float* l_s = Ls + (size_t)(kt % TGT_ST) * TGT_BK * TGT_LDB;
-    // the stage's 16-wide K step in a fresh accumulator; the three products of each step go out
-    // fragment by fragment (8 independent accumulators between dependent MMAs)
-    float d[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-#pragma unroll
-        for (int e = 0; e < 4; e++) d[i][j][e] = 0.f;
-#pragma unroll
-    for (int ks = 0; ks < TGT_BK; ks += 8) {
-      uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
-#pragma unroll
-      for (int i = 0; i < 2; i++) {
-        const float* ar = a_s + (32 * wm + 16 * i + g) * TGT_LDA + ks + t;
-        split_tf32(ar[0], ah[i][0], al[i][0]);
-        split_tf32(ar[8 * TGT_LDA], ah[i][1], al[i][1]);
-        split_tf32(ar[4], ah[i][2], al[i][2]);
-        split_tf32(ar[8 * TGT_LDA + 4], ah[i][3], al[i][3]);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int o = (ks + t) * TGT_LDB + 32 * wn + 8 * j + g;
-        bh[j][0] = __float_as_uint(h_s[o]);
-        bh[j][1] = __float_as_uint(h_s[o + 4 * TGT_LDB]);
-        bl[j][0] = __float_as_uint(l_s[o]);
-        bl[j][1] = __float_as_uint(l_s[o + 4 * TGT_LDB]);
-      }
-#pragma unroll
-      for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) mma_tf32_16x8x8(d[i][j], al[i], bh[j][0], bh[j][1]);
-#pragma unroll
-      for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) mma_tf32_16x8x8(d[i][j], ah[i], bl[j][0], bl[j][1]);
-#pragma unroll
-      for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) mma_tf32_16x8x8(d[i][j], ah[i], bh[j][0], bh[j][1]);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-#pragma unroll
-        for (int e = 0; e < 4; e++) run[i][j][e] = __fadd_rn(run[i][j][e], d[i][j][e]);
-  }
-  cp_wait<0>();
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int hr = 0; hr < 2; hr++) {
-      const int r = m0 + 32 * wm + 16 * i + g + 8 * hr;
-      if (r >= M) continue;
-      const double al = alpha ? alpha[r] : 1.0;
-      TC* crow = C + coff[r];
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const int col = n0 + 32 * wn + 8 * j + 2 * t + h;
-          if (col < N) store_out(crow + col, al * (double)run[i][j][2 * hr + h], acc);
-        }
-    }
-}
-
 // ---------------------------------------------------------------- FP32 accuracy on tcgen05 (TF32 x 3)
-// The same C = alpha A B as k_tgemm_tf32 on the sm_100 tensor cores.  A CTA owns 128 rows (one per TMEM
+// C = alpha A B on the sm_100 tensor cores (tcgen05).  A CTA owns 128 rows (one per TMEM
 // lane), 64 columns and a range of 16-wide K steps (K split over blockIdx.z when a level has few rows;
 // the parts are then added into C with atomics, C already holding the rows' starting values).
 // Per step: the rows' A pieces arrive raw by cp.async two steps ahead (16 bytes per lane, coalesced), in
@@ -688,23 +554,6 @@ void tgemm_f64(const TGemm& g, const TA* A, const double* B, TC* C, cudaStream_t
   XLAUNCH();
 }
 template <class TC>
-void tgemm_tf32(const TGemm& g, const float* A, const float* Bh, const float* Bl, TC* C, cudaStream_t s) {
-  if (g.M <= 0 || g.N <= 0) return;
-  const dim3 grid((g.M + TG_BM - 1) / TG_BM, (g.N + TG_BN - 1) / TG_BN);
-  // A rows (offsets multiples of astep floats) and B rows (ldb floats) 16-byte aligned when those are
-  // multiples of 4, else 8-byte copies (both at least 8-byte aligned)
-  XREQUIRE(g.ldb % 2 == 0 && g.astep % 2 == 0, XFMM_ERR_UNSUPPORTED, "translation rows must be 8-byte aligned");
-  const bool v16 = g.astep % 4 == 0 && g.ldb % 4 == 0;
-  auto go = [&](auto kern) {
-    XCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TGT_SMEM));
-    kern<<<grid, TG_NT, TGT_SMEM, s>>>(g.M, g.N, g.K, A, g.aoff, Bh, Bl, g.ldb, g.alpha, C, g.coff, g.accumulate);
-  };
-  if (v16) go(k_tgemm_tf32<TC, 16>);
-  else go(k_tgemm_tf32<TC, 8>);
-  XLAUNCH();
-}
-
-template <class TC>
 void tgemm_tc(const TGemm& g, const float* A, const float* Bth, const float* Btl, int64_t ldbt, TC* C,
               cudaStream_t s) {
   if (g.M <= 0 || g.N <= 0) return;
@@ -767,8 +616,6 @@ template void tgemm_f64<float, float>(const TGemm&, const float*, const double*,
 template void tgemm_f64<float, double>(const TGemm&, const float*, const double*, double*, cudaStream_t);
 template void tgemm_f64<double, float>(const TGemm&, const double*, const double*, float*, cudaStream_t);
 template void tgemm_f64<double, double>(const TGemm&, const double*, const double*, double*, cudaStream_t);
-template void tgemm_tf32<float>(const TGemm&, const float*, const float*, const float*, float*, cudaStream_t);
-template void tgemm_tf32<double>(const TGemm&, const float*, const float*, const float*, double*, cudaStream_t);
 
 }  // namespace xfmm
 

@@ -236,8 +236,6 @@ struct TGemm {
 template <class TA, class TC>
 void tgemm_f64(const TGemm& g, const TA* A, const double* B, TC* C, cudaStream_t s);
 template <class TC>
-void tgemm_tf32(const TGemm& g, const float* A, const float* Bh, const float* Bl, TC* C, cudaStream_t s);
-template <class TC>
 void tgemm_tc(const TGemm& g, const float* A, const float* Bth, const float* Btl, int64_t ldbt, TC* C,
               cudaStream_t s);
 int64_t tgemm_tc_scratch(int M, int N, int K, int accumulate);
