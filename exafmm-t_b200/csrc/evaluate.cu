@@ -3351,7 +3351,10 @@ Batch* batch_create(Fmm** fmms, Tree** trees, int n, cudaStream_t s) {
         for (int j = 0; j < ws.had_tile0[1] - ws.had_tile0[0]; j++) tl.push_back(make_int2(k, j));
       }
       // per-level translations over all systems' rows: offsets rebased onto system 0's up / dn arrays (every
-      // system's arrays are separate allocations, 256-byte aligned: the rebased offsets keep 16-byte rows)
+      // system's arrays are separate allocations, 256-byte aligned: the rebased offsets keep 16-byte rows).
+      // A rebased offset reaches from system 0's array into another system's allocation: this relies on the
+      // device's single flat address space (every allocation of the context is addressed from one base),
+      // not on C++ pointer rules, and the offsets are only ever applied on the device.
       int maxd = 0;
       for (int k = 0; k < n; k++) maxd = std::max(maxd, trees[k]->depth);
       const int prec = fmms[0]->precision, ns = fmms[0]->nsurf;
